@@ -1,0 +1,768 @@
+// kernels.cuh -- node-parallel kernels of the femh engine: coefficients, the
+// strain-driven right-hand sides, fused CG vector updates with FP64 partial
+// sums, per-(cell, load case) scalar finalisation, multigrid transfers, the
+// dense FP64 coarse solve, and the FP64 energy reductions (C^H, dC^H/drho,
+// dL/drho).
+//
+// All node-parallel kernels take a NodeUnit table: one CTA per (unit, load
+// case), a unit being a contiguous node range of one cell, so that thousands
+// of cells of different sizes run in the same launch.
+#pragma once
+#include "femh_common.cuh"
+#include "stencil.cuh"
+
+namespace femh {
+
+// Material law of the per-voxel modulus E(rho) (K0 is built for E = 1).
+enum Interp : int { INTERP_SIMP = 0, INTERP_RAMP3 = 1, INTERP_BINARY = 2 };
+struct MatLaw {
+  int interp;
+  int rho_bf16;   // round rho to bf16 before the law (mixed-precision option)
+  double E_s, E_min, penal, bin_hi, bin_lo, rho_min, rho_max;
+};
+
+__host__ __device__ inline double law_coef(const MatLaw& m, double rho) {
+  if (m.interp == INTERP_SIMP) return m.E_min + pow(rho, m.penal) * (m.E_s - m.E_min);
+  if (m.interp == INTERP_RAMP3) return m.E_s * rho / (3.0 - 2.0 * rho);
+  return rho >= 0.5 ? m.bin_hi : m.bin_lo;
+}
+__host__ __device__ inline double law_dcoef(const MatLaw& m, double rho) {
+  if (m.interp == INTERP_SIMP) return m.penal * pow(rho, m.penal - 1.0) * (m.E_s - m.E_min);
+  if (m.interp == INTERP_RAMP3) {
+    const double d = 3.0 - 2.0 * rho;
+    return m.E_s * 3.0 / (d * d);
+  }
+  return 0.0;
+}
+
+// Constants of the load and energy kernels, for h = 1 (scaled by h inside).
+struct ElemConst {
+  double g1[kNumRhs][24];      // K0(E=1,h=1) ue0^I(h=1), DOF 3a+c
+  double uhat0[kNumRhs][3][8]; // Hadamard transform of ue0^I(h=1)
+};
+
+__device__ __forceinline__ void node_ijk(long long n, int ny, int nz, int& i, int& j, int& k) {
+  const long long p = (long long)ny * nz;
+  i = (int)(n / p);
+  const long long rem = n - (long long)i * p;
+  j = (int)(rem / nz);
+  k = (int)(rem - (long long)j * nz);
+}
+__device__ __forceinline__ long long lin(int i, int j, int k, int ny, int nz) {
+  return ((long long)i * ny + j) * nz + k;
+}
+__device__ __forceinline__ int wrap(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
+
+// ---------------------------------------------------------------- setup ---
+// Fine-level stiffness scale kc[e] = E(clamp(rho_e)) * h and the rho actually used.
+template <typename TC2>
+__global__ void k_coef(const CellDesc* cells, const NodeUnit* units, const double* rho, MatLaw law,
+                       double* kc64, TC2* kc2, double* rho_used) {
+  const NodeUnit u = units[blockIdx.x];
+  const CellDesc cd = cells[u.cell];
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+    double r = rho[cd.off + n];
+    r = fmin(fmax(r, law.rho_min), law.rho_max);
+    if (law.rho_bf16) r = (double)__bfloat162float(__float2bfloat16_rn((float)r));
+    const double kc = law_coef(law, r) * cd.h;
+    if (rho_used) rho_used[cd.off + n] = r;
+    if (kc64) kc64[cd.off + n] = kc;
+    if (kc2) kc2[cd.off + n] = (TC2)kc;
+  }
+}
+
+// Rediscretised coarse scale: coarse voxel E = mean of its 8 children, voxel
+// edge 2h, so kc_c = (1/8) sum kc_f * 2 = (1/4) sum kc_f.
+template <typename TF, typename TCo>
+__global__ void k_coarsen_coef(const CellDesc* fine, const CellDesc* coarse, const NodeUnit* units,
+                               const TF* kcf, TCo* kcc) {
+  const NodeUnit u = units[blockIdx.x];
+  const CellDesc cc = coarse[u.cell], cf = fine[cc.parent];
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+    int i, j, k;
+    node_ijk(n, cc.ny, cc.nz, i, j, k);
+    double s = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+      s += (double)kcf[cf.off + lin(2 * i + ((a >> 2) & 1), 2 * j + ((a >> 1) & 1), 2 * k + (a & 1),
+                                    cf.ny, cf.nz)];
+    kcc[cc.off + n] = (TCo)(0.25 * s);
+  }
+}
+
+// Point-Jacobi inverse diagonal: all 24 diagonal entries of the cube's K0 are
+// equal, so diag(K)_n = K0diag * sum_{8 voxels at n} kc_e for all 3 components.
+template <typename TC>
+__global__ void k_invdiag(const CellDesc* cells, const NodeUnit* units, const TC* kc, double diag,
+                          float* invd) {
+  const NodeUnit u = units[blockIdx.x];
+  const CellDesc cd = cells[u.cell];
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+    int i, j, k;
+    node_ijk(n, cd.ny, cd.nz, i, j, k);
+    double s = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+      s += (double)kc[cd.off + lin(wrap(i - ((a >> 2) & 1), cd.nx), wrap(j - ((a >> 1) & 1), cd.ny),
+                                   wrap(k - (a & 1), cd.nz), cd.ny, cd.nz)];
+    invd[cd.off + n] = (n == 0) ? 0.f : (float)(1.0 / (diag * s));
+  }
+}
+
+// Strain-driven load b^I_n = -sum_{e at n} c_e (K0(h) ue0^I(h))[a_n(e)]
+//   = -h * sum_e kc_e g1^I[a_n(e)]  (K0(h) = h K0(1), ue0(h) = h ue0(1), kc = c h).
+// Pinned node 0 gets 0.  One CTA per (unit, load case).
+template <typename TB>
+__global__ void k_rhs(const CellDesc* cells, const NodeUnit* units, const double* kc64,
+                      const ElemConst* ec, TB* b, long long ntot) {
+  const NodeUnit u = units[blockIdx.x];
+  const int I = blockIdx.y;
+  const CellDesc cd = cells[u.cell];
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+    int i, j, k;
+    node_ijk(n, cd.ny, cd.nz, i, j, k);
+    double acc[3] = {0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const double ke = kc64[cd.off + lin(wrap(i - ((a >> 2) & 1), cd.nx), wrap(j - ((a >> 1) & 1), cd.ny),
+                                          wrap(k - (a & 1), cd.nz), cd.ny, cd.nz)];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc[c] += ke * ec->g1[I][3 * a + c];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      st_val(b + ((long long)I * 3 + c) * ntot + cd.off + n, (n == 0) ? 0.0 : -cd.h * acc[c]);
+  }
+}
+
+// ------------------------------------------------------------- CG pieces ---
+// Start of PCG: x = 0, r = s*b (s = per (cell,rhs) scale), partial ||r||^2.
+// With jacobi != 0 also partial r.(invd r) for the Jacobi-preconditioned rz and
+// p = invd r.  Partials: [slot][6][2].
+template <typename TB, typename TV, typename TP>
+__global__ void k_cg_init(const CellDesc* cells, const NodeUnit* units, const TB* b, TV* x, TV* r,
+                          TP* p, const float* invd, const CGState* stt, double* part, long long ntot,
+                          int jacobi) {
+  const NodeUnit u = units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cd = cells[u.cell];
+  const CGState S = stt[cd.id * kNumRhs + rhs];
+  double v[2] = {0.0, 0.0};
+  if (S.active) {
+    for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+      const long long g = cd.off + n;
+      const float id = invd[g];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const long long o = ((long long)rhs * 3 + c) * ntot + g;
+        const double rv = (n == 0) ? 0.0 : S.scale * (double)ld_val(b + o);
+        st_val(x + o, 0.0);
+        st_val(r + o, rv);
+        v[0] += rv * rv;
+        if (jacobi) {
+          const double z = (double)id * rv;
+          v[1] += rv * z;
+          st_val(p + o, z);
+        }
+      }
+    }
+  }
+  __shared__ double red[64];
+  block_reduce<2>(v, red);
+  if (threadIdx.x == 0) {
+    part[((long long)u.slot * kNumRhs + rhs) * 2 + 0] = v[0];
+    part[((long long)u.slot * kNumRhs + rhs) * 2 + 1] = v[1];
+  }
+}
+
+// x += alpha p ; r -= alpha q (r = 0 at node 0) ; partial ||r||^2 and, for
+// Jacobi, r.(invd r).  For the multigrid preconditioner (z0 != nullptr) it
+// also writes the first damped-Jacobi sweep from zero: z0 = omega invd r.
+template <typename TV, typename TP, typename TQ, typename TZ>
+__global__ void k_cg_update(const CellDesc* cells, const NodeUnit* units, TV* x, TV* r, const TP* p,
+                            const TQ* q, const float* invd, TZ* z0, double omega, const CGState* stt,
+                            double* part, long long ntot) {
+  const NodeUnit u = units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cd = cells[u.cell];
+  const CGState S = stt[cd.id * kNumRhs + rhs];
+  double v[2] = {0.0, 0.0};
+  if (S.active) {
+    const double al = S.alpha;
+    for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+      const long long g = cd.off + n;
+      const double id = (double)invd[g];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const long long o = ((long long)rhs * 3 + c) * ntot + g;
+        const double pv = (double)ld_val(p + o);
+        const double xv = (double)ld_val(x + o) + al * pv;
+        const double rv = (n == 0) ? 0.0 : (double)ld_val(r + o) - al * (double)ld_val(q + o);
+        st_val(x + o, xv);
+        st_val(r + o, rv);
+        v[0] += rv * rv;
+        v[1] += rv * id * rv;
+        if (z0) st_val(z0 + o, omega * id * rv);
+      }
+    }
+  }
+  __shared__ double red[64];
+  block_reduce<2>(v, red);
+  if (threadIdx.x == 0) {
+    part[((long long)u.slot * kNumRhs + rhs) * 2 + 0] = v[0];
+    part[((long long)u.slot * kNumRhs + rhs) * 2 + 1] = v[1];
+  }
+}
+
+// p = z + beta p, with z = invd r (Jacobi) or z read from zvec (multigrid).
+template <typename TP, typename TZ, typename TR>
+__global__ void k_cg_dir(const CellDesc* cells, const NodeUnit* units, TP* p, const TZ* zvec,
+                         const TR* r, const float* invd, const CGState* stt, long long ntot) {
+  const NodeUnit u = units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cd = cells[u.cell];
+  const CGState S = stt[cd.id * kNumRhs + rhs];
+  if (!S.active) return;
+  const double be = S.beta;
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+    const long long g = cd.off + n;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long o = ((long long)rhs * 3 + c) * ntot + g;
+      const double z = zvec ? (double)ld_val(zvec + o) : (double)invd[g] * (double)ld_val(r + o);
+      st_val(p + o, z + be * (double)ld_val(p + o));
+    }
+  }
+}
+
+// Sum of the partials of one (cell, rhs) over the cell's slot range, fixed order.
+__device__ __forceinline__ double sum_slots(const double* part, int b, int e, int rhs, int stride,
+                                            int comp) {
+  double s = 0.0;
+  for (int t = b; t < e; ++t) s += part[((long long)t * kNumRhs + rhs) * stride + comp];
+  return s;
+}
+
+// After k_cg_init: bnorm2, rz (Jacobi) / rr; decide which (cell, rhs) run.
+// One thread per (cell, rhs).
+__global__ void k_fin_init(CGState* stt, const int* slot_begin, const int* slot_end,
+                           const double* part, int ncells, int jacobi) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncells * kNumRhs) return;
+  const int cell = t / kNumRhs, rhs = t % kNumRhs;
+  CGState S = stt[t];
+  if (!S.active) return;
+  const double rr = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 2, 0);
+  S.bnorm2 = rr;
+  S.rr = rr;
+  S.rz = jacobi ? sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 2, 1) : 0.0;
+  S.iters = 0;
+  S.rel = (rr > 0.0) ? 1.0 : 0.0;
+  if (!(rr > 0.0)) { S.active = 0; S.status = CG_CONVERGED; }
+  stt[t] = S;
+}
+
+// rz for the multigrid preconditioner at start (z0 . r from the V-cycle's last sweep).
+__global__ void k_fin_rz(CGState* stt, const int* slot_begin, const int* slot_end,
+                         const double* part, int ncells) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncells * kNumRhs) return;
+  const int cell = t / kNumRhs, rhs = t % kNumRhs;
+  CGState S = stt[t];
+  if (!S.active) return;
+  S.rz = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 1, 0);
+  stt[t] = S;
+}
+
+// alpha = rz / (p . K p); breakdown if p.Kp <= 0 or not finite.
+__global__ void k_fin_alpha(CGState* stt, const int* slot_begin, const int* slot_end,
+                            const double* part, int ncells) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncells * kNumRhs) return;
+  const int cell = t / kNumRhs, rhs = t % kNumRhs;
+  CGState S = stt[t];
+  if (!S.active) return;
+  const double pq = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 1, 0);
+  S.pq = pq;
+  if (!(pq > 0.0) || !isfinite(pq) || !isfinite(S.rz)) {
+    S.alpha = 0.0;
+    S.active = 0;
+    S.status = CG_BREAKDOWN;
+  } else {
+    S.alpha = S.rz / pq;
+  }
+  stt[t] = S;
+}
+
+// After the update (+ preconditioner): convergence test and beta.
+// jacobi: rz_new from the update partials; else from the V-cycle partials.
+__global__ void k_fin_beta(CGState* stt, const int* slot_begin, const int* slot_end,
+                           const double* part_upd, const double* part_rz, int ncells, int jacobi) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncells * kNumRhs) return;
+  const int cell = t / kNumRhs, rhs = t % kNumRhs;
+  CGState S = stt[t];
+  if (!S.active) return;
+  const int b = slot_begin[cell], e = slot_end[cell];
+  const double rr = sum_slots(part_upd, b, e, rhs, 2, 0);
+  const double rzn = jacobi ? sum_slots(part_upd, b, e, rhs, 2, 1) : sum_slots(part_rz, b, e, rhs, 1, 0);
+  S.rr = rr;
+  S.iters += 1;
+  S.rel = sqrt(rr / S.bnorm2);
+  if (S.rel < S.tol) {
+    S.active = 0;
+    S.status = CG_CONVERGED;
+  } else if (S.iters >= S.max_iter) {
+    S.active = 0;
+    S.status = CG_MAXITER;
+  } else if (!isfinite(rzn) || !(rzn > 0.0)) {
+    S.active = 0;
+    S.status = CG_BREAKDOWN;
+  } else {
+    S.beta = rzn / S.rz;
+    S.rz = rzn;
+  }
+  stt[t] = S;
+}
+
+// ---------------------------------------------------------- multigrid ---
+// Full-weighting restriction (transpose of trilinear prolongation):
+// bc(I) = sum_{d in {-1,0,1}^3} prod_s (1 - |d_s|/2) rf(2I + d); 0 at node 0.
+template <typename TF, typename TCo>
+__global__ void k_restrict(const CellDesc* fine, const CellDesc* coarse, const NodeUnit* units,
+                           const TF* rf, TCo* bc, const CGState* stt, long long ntf, long long ntc) {
+  const NodeUnit u = units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cc = coarse[u.cell], cf = fine[cc.parent];
+  if (stt && !stt[cc.id * kNumRhs + rhs].active) return;
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+    int i, j, k;
+    node_ijk(n, cc.ny, cc.nz, i, j, k);
+    double acc[3] = {0, 0, 0};
+    if (n != 0) {
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int fi = wrap(2 * i + dx, cf.nx);
+        const double wx = dx ? 0.5 : 1.0;
+        for (int dy = -1; dy <= 1; ++dy) {
+          const int fj = wrap(2 * j + dy, cf.ny);
+          const double wy = wx * (dy ? 0.5 : 1.0);
+#pragma unroll
+          for (int dz = -1; dz <= 1; ++dz) {
+            const int fk = wrap(2 * k + dz, cf.nz);
+            const double w = wy * (dz ? 0.5 : 1.0);
+            const long long g = cf.off + lin(fi, fj, fk, cf.ny, cf.nz);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[c] += w * (double)ld_val(rf + ((long long)rhs * 3 + c) * ntf + g);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) st_val(bc + ((long long)rhs * 3 + c) * ntc + cc.off + n, acc[c]);
+  }
+}
+
+// Trilinear prolongation and correction: xf(n) += sum_I w(n,I) ec(I).
+template <typename TF, typename TCo>
+__global__ void k_prolong_add(const CellDesc* fine, const CellDesc* coarse, const NodeUnit* units,
+                              TF* xf, const TCo* ec, const CGState* stt, long long ntf, long long ntc) {
+  const NodeUnit u = units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cf = fine[u.cell], cc = coarse[fine[u.cell].child];
+  if (stt && !stt[cf.id * kNumRhs + rhs].active) return;
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+    int i, j, k;
+    node_ijk(n, cf.ny, cf.nz, i, j, k);
+    const int ci0 = i >> 1, cj0 = j >> 1, ck0 = k >> 1;
+    const int nxi = (i & 1) ? 2 : 1, nyj = (j & 1) ? 2 : 1, nzk = (k & 1) ? 2 : 1;
+    const double wx = (i & 1) ? 0.5 : 1.0, wy = (j & 1) ? 0.5 : 1.0, wz = (k & 1) ? 0.5 : 1.0;
+    double acc[3] = {0, 0, 0};
+    for (int a = 0; a < nxi; ++a)
+      for (int b = 0; b < nyj; ++b)
+        for (int d = 0; d < nzk; ++d) {
+          const long long g = cc.off + lin(wrap(ci0 + a, cc.nx), wrap(cj0 + b, cc.ny), wrap(ck0 + d, cc.nz),
+                                           cc.ny, cc.nz);
+          const double w = wx * wy * wz;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) acc[c] += w * (double)ld_val(ec + ((long long)rhs * 3 + c) * ntc + g);
+        }
+    if (n == 0) continue;   // pinned node keeps 0
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      TF* px = xf + ((long long)rhs * 3 + c) * ntf + cf.off + n;
+      st_val(px, (double)ld_val(px) + acc[c]);
+    }
+  }
+}
+
+// z = omega * invd * b  (first damped-Jacobi sweep from a zero start)
+template <typename TB, typename TX>
+__global__ void k_jacobi0(const CellDesc* cells, const NodeUnit* units, const TB* b, TX* x,
+                          const float* invd, double omega, const CGState* stt, long long ntot) {
+  const NodeUnit u = units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cd = cells[u.cell];
+  if (stt && !stt[cd.id * kNumRhs + rhs].active) return;
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+    const long long g = cd.off + n;
+    const double id = (double)invd[g];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long o = ((long long)rhs * 3 + c) * ntot + g;
+      st_val(x + o, omega * id * (double)ld_val(b + o));
+    }
+  }
+}
+
+// Dense coarse operator of one cell (one CTA per cell), FP64: A = sum_e kc_e K0(1)
+// scattered to the periodic DOFs; the 3 DOFs of node 0 are replaced by identity
+// rows/columns (pinned).  A is m x m, m = 3 * nodes.
+template <typename TC>
+__global__ void k_coarse_assemble(const CellDesc* cells, const int* list, const TC* kc,
+                                  const double* K0, double* A, const long long* aoff) {
+  const CellDesc cd = cells[list[blockIdx.x]];
+  const long long nn = (long long)cd.nx * cd.ny * cd.nz;
+  const int m = (int)(3 * nn);
+  double* M = A + aoff[blockIdx.x];
+  for (long long t = threadIdx.x; t < (long long)m * m; t += blockDim.x) M[t] = 0.0;
+  __syncthreads();
+  for (long long e = 0; e < nn; ++e) {
+    int i, j, k;
+    node_ijk(e, cd.ny, cd.nz, i, j, k);
+    const double ke = (double)kc[cd.off + e];
+    for (int t = threadIdx.x; t < 576; t += blockDim.x) {
+      const int p = t / 24, q = t % 24;
+      const int ap = p / 3, cp = p % 3, aq = q / 3, cq = q % 3;
+      const long long np = lin(wrap(i + ((ap >> 2) & 1), cd.nx), wrap(j + ((ap >> 1) & 1), cd.ny),
+                               wrap(k + (ap & 1), cd.nz), cd.ny, cd.nz);
+      const long long nq = lin(wrap(i + ((aq >> 2) & 1), cd.nx), wrap(j + ((aq >> 1) & 1), cd.ny),
+                               wrap(k + (aq & 1), cd.nz), cd.ny, cd.nz);
+      M[(3 * np + cp) * m + 3 * nq + cq] += ke * K0[t];
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < m; t += blockDim.x)
+    for (int c = 0; c < 3; ++c) {
+      M[(long long)c * m + t] = (t == c) ? 1.0 : 0.0;
+      M[(long long)t * m + c] = (t == c) ? 1.0 : 0.0;
+    }
+}
+
+// In-place Cholesky A = L L^T, then A <- A^{-1} (explicit SPD inverse, FP64),
+// one CTA per cell.  work holds m*m doubles per cell.  status[cell] = 0 ok,
+// k+1 if pivot k was not positive.
+__global__ void k_coarse_factor(const CellDesc* cells, const int* list, double* A, double* work,
+                                const long long* aoff, int* status) {
+  const CellDesc cd = cells[list[blockIdx.x]];
+  const int m = 3 * cd.nx * cd.ny * cd.nz;
+  double* L = A + aoff[blockIdx.x];
+  double* X = work + aoff[blockIdx.x];
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  for (int k = 0; k < m; ++k) {
+    if (threadIdx.x == 0) {
+      const double d = L[(long long)k * m + k];
+      if (!(d > 0.0) && !bad) bad = k + 1;
+      L[(long long)k * m + k] = sqrt(fmax(d, 1e-300));
+    }
+    __syncthreads();
+    const double dk = L[(long long)k * m + k];
+    for (int i = k + 1 + threadIdx.x; i < m; i += blockDim.x) L[(long long)i * m + k] /= dk;
+    __syncthreads();
+    for (long long t = threadIdx.x; t < (long long)(m - k - 1) * (m - k - 1); t += blockDim.x) {
+      const int i = k + 1 + (int)(t / (m - k - 1)), j = k + 1 + (int)(t % (m - k - 1));
+      if (j <= i) L[(long long)i * m + j] -= L[(long long)i * m + k] * L[(long long)j * m + k];
+    }
+    __syncthreads();
+  }
+  // X = A^{-1}: solve L L^T X = I column by column (threads over columns)
+  for (int col = threadIdx.x; col < m; col += blockDim.x) {
+    for (int i = 0; i < m; ++i) {   // forward: L y = e_col
+      double s = (i == col) ? 1.0 : 0.0;
+      for (int j = 0; j < i; ++j) s -= L[(long long)i * m + j] * X[(long long)j * m + col];
+      X[(long long)i * m + col] = s / L[(long long)i * m + i];
+    }
+    for (int i = m - 1; i >= 0; --i) {   // backward: L^T x = y
+      double s = X[(long long)i * m + col];
+      for (int j = i + 1; j < m; ++j) s -= L[(long long)j * m + i] * X[(long long)j * m + col];
+      X[(long long)i * m + col] = s / L[(long long)i * m + i];
+    }
+  }
+  __syncthreads();
+  for (long long t = threadIdx.x; t < (long long)m * m; t += blockDim.x) L[t] = X[t];
+  if (threadIdx.x == 0) status[blockIdx.x] = bad;
+}
+
+// Coarse solve e = A^{-1} b for one (cell, rhs) per CTA (A^{-1} symmetric).
+template <typename TB, typename TX>
+__global__ void k_coarse_solve(const CellDesc* cells, const int* list, const double* Ainv,
+                               const long long* aoff, const TB* b, TX* x, const CGState* stt,
+                               long long ntot) {
+  const int cell = list[blockIdx.x], rhs = blockIdx.y;
+  const CellDesc cd = cells[cell];
+  if (stt && !stt[cd.id * kNumRhs + rhs].active) return;
+  const int nn = cd.nx * cd.ny * cd.nz, m = 3 * nn;
+  extern __shared__ double sb[];
+  for (int t = threadIdx.x; t < m; t += blockDim.x) {
+    const int n = t / 3, c = t % 3;
+    sb[t] = (double)ld_val(b + ((long long)rhs * 3 + c) * ntot + cd.off + n);
+  }
+  __syncthreads();
+  const double* M = Ainv + aoff[blockIdx.x];
+  for (int t = threadIdx.x; t < m; t += blockDim.x) {
+    double s = 0.0;
+    for (int j = 0; j < m; ++j) s += M[(long long)j * m + t] * sb[j];
+    const int n = t / 3, c = t % 3;
+    st_val(x + ((long long)rhs * 3 + c) * ntot + cd.off + n, (n == 0) ? 0.0 : s);
+  }
+}
+
+// ------------------------------------------------------- energy kernels ---
+// Per voxel: u^I = ue0^I(h) + chi^I (6 load cases), uhat = T u, w = Kh uhat;
+// s_IJ = uhat^I . w^J = u^I . K0(1) u^J.  Modes:
+//   C partials:   sum_e kc_e s_IJ       (-> C^H = sum / (|Y|))     [slot][21]
+//   dC/drho:      out[t][e] = c'(rho_e) h s_t / |Y|
+//   dL/drho:      out[e] = c'(rho_e) h sum_t W_t s_t / |Y|
+enum EnergyMode : int { EN_C = 0, EN_DCDRHO = 1, EN_GRAD = 2 };
+struct EnergyArgs {
+  const CellDesc* cells;
+  const NodeUnit* units;
+  const double* chi;      // [6][3][ntot] FP64
+  const double* kc64;     // c_e * h
+  const double* rho;      // rho actually used (clamped)
+  const ElemConst* ec;
+  const double* W;        // [cell][21] symmetric weights for EN_GRAD
+  double* part;           // EN_C: [slot][21]
+  double* out;            // EN_DCDRHO: [21][ntot]; EN_GRAD: [ntot]
+  long long ntot;
+  HadK k;
+  MatLaw law;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_energy(EnergyArgs a) {
+  const NodeUnit u = a.units[blockIdx.x];
+  const CellDesc cd = a.cells[u.cell];
+  const double vol = (double)cd.nx * cd.ny * cd.nz * cd.h * cd.h * cd.h;
+  double acc[22];
+#pragma unroll
+  for (int t = 0; t < 22; ++t) acc[t] = 0.0;
+  for (long long e = u.begin + threadIdx.x; e < u.end; e += blockDim.x) {
+    int i, j, k;
+    node_ijk(e, cd.ny, cd.nz, i, j, k);
+    long long nd[8];
+#pragma unroll
+    for (int a8 = 0; a8 < 8; ++a8)
+      nd[a8] = cd.off + lin(wrap(i + ((a8 >> 2) & 1), cd.nx), wrap(j + ((a8 >> 1) & 1), cd.ny),
+                            wrap(k + (a8 & 1), cd.nz), cd.ny, cd.nz);
+    double uh[kNumRhs][3][8];
+#pragma unroll
+    for (int I = 0; I < kNumRhs; ++I)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+#pragma unroll
+        for (int a8 = 0; a8 < 8; ++a8) uh[I][c][a8] = a.chi[((long long)I * 3 + c) * a.ntot + nd[a8]];
+        fwht8_fwd(uh[I][c]);
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) uh[I][c][kk] += cd.h * a.ec->uhat0[I][c][kk];
+      }
+    double s[21];
+#pragma unroll
+    for (int J = 0; J < kNumRhs; ++J) {
+      double w[3][8];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) w[c][kk] = uh[J][c][kk];
+      had_block(w, a.k, 1.0);
+#pragma unroll
+      for (int I = J; I < kNumRhs; ++I) {
+        double d = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int kk = 1; kk < 8; ++kk) d += uh[I][c][kk] * w[c][kk];
+        s[I * (I + 1) / 2 + J] = d;   // u^I.K0 u^J = (T u^I).Kh (T u^J)
+      }
+    }
+    if (MODE == EN_C) {
+      const double ke = a.kc64[cd.off + e];
+#pragma unroll
+      for (int t = 0; t < 21; ++t) acc[t] += ke * s[t];
+      acc[21] += a.rho[cd.off + e];
+    } else {
+      const double dc = law_dcoef(a.law, a.rho[cd.off + e]) * cd.h / vol;
+      if (MODE == EN_DCDRHO) {
+#pragma unroll
+        for (int t = 0; t < 21; ++t) a.out[(long long)t * a.ntot + cd.off + e] = dc * s[t];
+      } else {
+        double g = 0.0;
+#pragma unroll
+        for (int t = 0; t < 21; ++t) g += a.W[cd.id * 21 + t] * s[t];
+        a.out[cd.off + e] = dc * g;
+      }
+    }
+  }
+  if (MODE == EN_C) {
+    __shared__ double red[32 * 22];
+    block_reduce<22>(acc, red);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int t = 0; t < 22; ++t) a.part[(long long)u.slot * 22 + t] = acc[t];
+  }
+}
+
+// C^H of each cell from its energy partials (fixed order), one thread per (cell, pair).
+__global__ void k_energy_fin(const CellDesc* cells, const int* slot_begin, const int* slot_end,
+                             const double* part, double* C, double* dens, int ncells) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncells * 22) return;
+  const int cell = t / 22, q = t % 22;
+  const CellDesc cd = cells[cell];
+  const double nvx = (double)cd.nx * cd.ny * cd.nz;
+  const double vol = nvx * cd.h * cd.h * cd.h;
+  double s = 0.0;
+  for (int sl = slot_begin[cell]; sl < slot_end[cell]; ++sl) s += part[(long long)sl * 22 + q];
+  if (q == 21) {
+    dens[cell] = s / nvx;
+    return;
+  }
+  int I = 0;
+  while ((I + 1) * (I + 2) / 2 <= q) ++I;
+  const int J = q - I * (I + 1) / 2;
+  C[cell * 36 + I * 6 + J] = s / vol;
+  C[cell * 36 + J * 6 + I] = s / vol;
+}
+
+// ------------------------------------------------------- misc vector ops ---
+// dst = src (cast), per load case, over all nodes of the units.
+template <typename TD, typename TS>
+__global__ void k_copy(const CellDesc* cells, const NodeUnit* units, TD* dst, const TS* src,
+                       const CGState* stt, long long ntot) {
+  const NodeUnit u = units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cd = cells[u.cell];
+  if (stt && !stt[cd.id * kNumRhs + rhs].active) return;
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long o = ((long long)rhs * 3 + c) * ntot + cd.off + n;
+      st_val(dst + o, (double)ld_val(src + o));
+    }
+}
+
+// Defect correction: x64 += d / scale (d from the inner solve).
+template <typename TD>
+__global__ void k_dc_accum(const CellDesc* cells, const NodeUnit* units, double* x64, const TD* d,
+                           const CGState* stt, long long ntot) {
+  const NodeUnit u = units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cd = cells[u.cell];
+  const CGState S = stt[cd.id * kNumRhs + rhs];
+  if (!S.active) return;
+  const double inv = 1.0 / S.scale;
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long o = ((long long)rhs * 3 + c) * ntot + cd.off + n;
+      x64[o] += inv * (double)ld_val(d + o);
+    }
+}
+
+
+// Partial a.b per (unit, rhs) into part[slot][6] (stride 1).
+template <typename TA, typename TB2>
+__global__ void k_dot(const CellDesc* cells, const NodeUnit* units, const TA* a, const TB2* b,
+                      const CGState* stt, double* part, long long ntot) {
+  const NodeUnit u = units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cd = cells[u.cell];
+  double acc[1] = {0.0};
+  if (!stt || stt[cd.id * kNumRhs + rhs].active) {
+    for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const long long o = ((long long)rhs * 3 + c) * ntot + cd.off + n;
+        acc[0] += (double)ld_val(a + o) * (double)ld_val(b + o);
+      }
+  }
+  __shared__ double red[32];
+  block_reduce<1>(acc, red);
+  if (threadIdx.x == 0) part[(long long)u.slot * kNumRhs + rhs] = acc[0];
+}
+
+// Partial ||v||^2 per (unit, rhs) into part[slot][6] (stride 1).
+template <typename TV>
+__global__ void k_norm2(const CellDesc* cells, const NodeUnit* units, const TV* v, double* part,
+                        long long ntot) {
+  const NodeUnit u = units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cd = cells[u.cell];
+  double acc[1] = {0.0};
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double x = (double)ld_val(v + ((long long)rhs * 3 + c) * ntot + cd.off + n);
+      acc[0] += x * x;
+    }
+  __shared__ double red[32];
+  block_reduce<1>(acc, red);
+  if (threadIdx.x == 0) part[(long long)u.slot * kNumRhs + rhs] = acc[0];
+}
+
+__global__ void k_sum_slots(const int* slot_begin, const int* slot_end, const double* part, double* out,
+                            int ncells) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncells * kNumRhs) return;
+  const int cell = t / kNumRhs, rhs = t % kNumRhs;
+  out[t] = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 1, 0);
+}
+
+// Full-cell displacement on (nx+1)(ny+1)(nz+1) nodes for load case I: periodic
+// chi plus the macro-strain affine field, the jump eps (X - X0) on the + faces
+// included (fast_fem/FEM3DFun.cpp:31-56 copyPeriodicU).  Layout [node][3].
+__global__ void k_full_field(const CellDesc* cells, int cell, const double* chi, int I, double* out,
+                             long long ntot) {
+  const CellDesc cd = cells[cell];
+  const int Nx = cd.nx + 1, Ny = cd.ny + 1, Nz = cd.nz + 1;
+  const long long total = (long long)Nx * Ny * Nz;
+  double eps[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  if (I < 3) eps[I][I] = 1.0;
+  if (I == 3) eps[1][2] = eps[2][1] = 0.5;
+  if (I == 4) eps[0][2] = eps[2][0] = 0.5;
+  if (I == 5) eps[0][1] = eps[1][0] = 0.5;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    node_ijk(t, Ny, Nz, i, j, k);
+    const long long n0 = cd.off + lin(i % cd.nx, j % cd.ny, k % cd.nz, cd.ny, cd.nz);
+    const double X[3] = {i * cd.h, j * cd.h, k * cd.h};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double aff = eps[c][0] * X[0] + eps[c][1] * X[1] + eps[c][2] * X[2];
+      out[3 * t + c] = chi[((long long)I * 3 + c) * ntot + n0] + aff;
+    }
+  }
+}
+
+}  // namespace femh
+
+namespace femh {
+// [6][3][node] (engine) <-> [6][node][3] (reference layout) for one cell.
+template <bool TO_AOS>
+__global__ void k_layout(const double* src, double* dst, long long off, long long nn, long long ntot) {
+  const long long total = nn * 18;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int I = (int)(t / (3 * nn));
+    const long long rem = t - (long long)I * 3 * nn;
+    const long long n = rem / 3;
+    const int c = (int)(rem - n * 3);
+    const long long eng = ((long long)I * 3 + c) * ntot + off + n;   // engine index
+    const long long ref = t;                                          // [I][n][c] of this cell
+    if (TO_AOS) dst[ref] = src[eng];
+    else dst[eng] = src[ref];
+  }
+}
+}  // namespace femh

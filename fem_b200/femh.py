@@ -1,0 +1,279 @@
+"""Python binding of libfemh (ctypes over the C ABI in include/femh.h).
+
+Thin by design: every numeric step runs in libfemh's CUDA kernels.  Loading
+fails loudly when the library is missing; there is no CPU fallback.
+
+Mirrors the reference's homogenization entry points (desaic/fem):
+``Engine.homogenize`` <-> FEM3DFun::setParam's solve + energy loop
+(fast_fem/FEM3DFun.cpp:128-196), ``Engine.grad`` <-> FEM3DFun::df
+(fast_fem/FEM3DFun.cpp:222-268), ``Engine.full_field`` <-> copyPeriodicU
+(fast_fem/FEM3DFun.cpp:31-56), ``Engine.batch`` <-> the sample generator's
+per-cell loop (SamplesGenerator/SamplesGeneratorImpl.cpp:3703-3736).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field, fields
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfemh.so")
+
+FEMH_OK, FEMH_E_ARG, FEMH_E_CUDA, FEMH_E_OOM, FEMH_E_NOT_CONVERGED, FEMH_E_BREAKDOWN, FEMH_E_STATE = range(7)
+INTERP_SIMP, INTERP_RAMP3, INTERP_BINARY = 0, 1, 2
+FP64, MIXED = 0, 1
+JACOBI_PCG, GMG_PCG = 0, 1
+
+#: every exported symbol of include/femh.h
+EXPORTS = (
+    "femh_config_default", "femh_create", "femh_destroy", "femh_homogenize", "femh_homogenize_grad",
+    "femh_dCdrho", "femh_full_field", "femh_fluctuation", "femh_apply_operator", "femh_homogenize_batch",
+    "femh_last_error", "femh_set_stream", "femh_kernel_launches",
+)
+
+
+class FemhError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"femh error {code}: {msg}")
+        self.code = code
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int), ("interp", ctypes.c_int),
+        ("E_s", ctypes.c_double), ("E_min", ctypes.c_double), ("penal", ctypes.c_double), ("nu", ctypes.c_double),
+        ("bin_hi", ctypes.c_double), ("bin_lo", ctypes.c_double),
+        ("rho_min", ctypes.c_double), ("rho_max", ctypes.c_double),
+        ("precision", ctypes.c_int), ("solver", ctypes.c_int),
+        ("pre_smooth", ctypes.c_int), ("post_smooth", ctypes.c_int),
+        ("omega", ctypes.c_double), ("coarse_max_nodes", ctypes.c_int),
+        ("tol", ctypes.c_double), ("max_iter", ctypes.c_int),
+        ("inner_tol", ctypes.c_double), ("max_outer", ctypes.c_int),
+        ("store_bf16", ctypes.c_int), ("graph_chunk", ctypes.c_int),
+    ]
+
+
+class _Info(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int), ("iterations", ctypes.c_int * 6), ("outer_iterations", ctypes.c_int),
+        ("rel_residual", ctypes.c_double * 6), ("solve_ms", ctypes.c_double), ("density", ctypes.c_double),
+    ]
+
+
+class _Cell(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("h", ctypes.c_double),
+                ("rho", ctypes.POINTER(ctypes.c_double))]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libfemh.so (build it with fem_b200/build.py first)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FemhError(FEMH_E_CUDA, f"{path} missing: run `python fem_b200/build.py` (no CPU fallback exists)")
+    L = ctypes.CDLL(path)
+    vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int
+    L.femh_config_default.argtypes = [ctypes.POINTER(_Config)]
+    L.femh_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(_Config)]
+    L.femh_destroy.argtypes = [vp]
+    L.femh_homogenize.argtypes = [vp, ip, ip, ip, ctypes.c_double, vp, ip, dp, ctypes.POINTER(_Info)]
+    L.femh_homogenize_grad.argtypes = [vp, dp, vp, ip]
+    L.femh_dCdrho.argtypes = [vp, vp, ip]
+    L.femh_full_field.argtypes = [vp, ip, vp, ip]
+    L.femh_fluctuation.argtypes = [vp, vp, ip]
+    L.femh_apply_operator.argtypes = [vp, ip, ip, ip, ctypes.c_double, vp, vp, vp, ip]
+    L.femh_homogenize_batch.argtypes = [vp, ip, ctypes.POINTER(_Cell), dp, vp, vp, ctypes.POINTER(_Info)]
+    L.femh_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    L.femh_set_stream.argtypes = [vp, vp]
+    L.femh_kernel_launches.argtypes = [vp]
+    L.femh_kernel_launches.restype = ctypes.c_longlong
+    _lib = L
+    return L
+
+
+@dataclass
+class Config:
+    """Engine configuration (fields of femh_config; defaults from femh_config_default)."""
+    device: int = 0
+    interp: int = INTERP_SIMP
+    E_s: float = 1.0
+    E_min: float = 1e-6
+    penal: float = 3.0
+    nu: float = 0.3
+    bin_hi: float = 1.0
+    bin_lo: float = 1e-4
+    rho_min: float = 0.0
+    rho_max: float = 1.0
+    precision: int = FP64
+    solver: int = GMG_PCG
+    pre_smooth: int = 2
+    post_smooth: int = 2
+    omega: float = 0.6
+    coarse_max_nodes: int = 64
+    tol: float = 1e-10
+    max_iter: int = 20000
+    inner_tol: float = 1e-5
+    max_outer: int = 8
+    store_bf16: int = 0
+    graph_chunk: int = 8
+
+    def to_c(self) -> _Config:
+        c = _Config()
+        for f in fields(self):
+            setattr(c, f.name, getattr(self, f.name))
+        return c
+
+
+def _info_dict(i: _Info) -> dict:
+    return {
+        "status": i.status, "iterations": list(i.iterations), "outer_iterations": i.outer_iterations,
+        "rel_residual": list(i.rel_residual), "solve_ms": i.solve_ms, "density": i.density,
+    }
+
+
+def _ptr(a) -> ctypes.c_void_p:
+    """Host numpy array or device torch tensor -> (pointer, on_device)."""
+    return ctypes.c_void_p(a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
+
+
+def _is_dev(a) -> int:
+    return 0 if isinstance(a, np.ndarray) else int(getattr(a, "is_cuda", False))
+
+
+class Engine:
+    """One libfemh handle (one CUDA stream)."""
+
+    def __init__(self, config: Optional[Config] = None, **kw):
+        self.lib = load_library()
+        self.config = config if config is not None else Config(**kw)
+        h = ctypes.c_void_p()
+        st = self.lib.femh_create(ctypes.byref(h), ctypes.byref(self.config.to_c()))
+        if st != FEMH_OK:
+            raise FemhError(st, "femh_create failed (no CUDA device or bad config)")
+        self.h = h
+        self.shape = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.femh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _err(self, st: int):
+        buf = ctypes.create_string_buffer(1024)
+        self.lib.femh_last_error(self.h, buf, 1024)
+        return FemhError(st, buf.value.decode())
+
+    def _check(self, st: int, allow=(FEMH_OK,)):
+        if st not in allow:
+            raise self._err(st)
+        return st
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.lib.femh_kernel_launches(self.h))
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(self.lib.femh_set_stream(self.h, ctypes.c_void_p(stream_ptr or 0)))
+
+    # ------------------------------------------------------------ forward
+    def homogenize(self, rho, h: float | None = None, allow_unconverged: bool = False):
+        """C^H (6x6 numpy) and the solve info of one periodic cell.
+
+        rho: (nx, ny, nz) float64 numpy array (host) or CUDA torch tensor."""
+        nx, ny, nz = (int(s) for s in rho.shape)
+        if isinstance(rho, np.ndarray):
+            rho = np.ascontiguousarray(rho, dtype=np.float64)
+        else:
+            assert rho.dtype.__str__() == "torch.float64" and rho.is_contiguous()
+        h = 1.0 / nx if h is None else float(h)
+        C = np.zeros((6, 6))
+        info = _Info()
+        st = self.lib.femh_homogenize(self.h, nx, ny, nz, h, _ptr(rho), _is_dev(rho),
+                                      C.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(info))
+        allow = (FEMH_OK, FEMH_E_NOT_CONVERGED, FEMH_E_BREAKDOWN) if allow_unconverged else (FEMH_OK,)
+        self._check(st, allow)
+        self.shape = (nx, ny, nz)
+        return C, _info_dict(info)
+
+    def grad(self, dLdC, out=None):
+        """dL/drho for dL/dC at the last solve (adjoint, no second solve)."""
+        dLdC = np.ascontiguousarray(dLdC, dtype=np.float64).reshape(6, 6)
+        if out is None:
+            out = np.zeros(self.shape)
+        self._check(self.lib.femh_homogenize_grad(self.h, dLdC.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                  _ptr(out), _is_dev(out)))
+        return out
+
+    def dCdrho(self, out=None):
+        """dC_IJ/drho_e for the 21 lower-triangle pairs: array [21, nx, ny, nz]."""
+        if out is None:
+            out = np.zeros((21,) + tuple(self.shape))
+        self._check(self.lib.femh_dCdrho(self.h, _ptr(out), _is_dev(out)))
+        return out
+
+    def full_field(self, load_case: int):
+        nx, ny, nz = self.shape
+        out = np.zeros((nx + 1, ny + 1, nz + 1, 3))
+        self._check(self.lib.femh_full_field(self.h, int(load_case), _ptr(out), 0))
+        return out
+
+    def fluctuation(self):
+        out = np.zeros((6,) + tuple(self.shape) + (3,))
+        self._check(self.lib.femh_fluctuation(self.h, _ptr(out), 0))
+        return out
+
+    def apply_operator(self, rho, u, h: float | None = None):
+        """y = K(rho) u for u of shape (6, nx, ny, nz, 3) (host float64)."""
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        nx, ny, nz = rho.shape
+        assert u.shape == (6, nx, ny, nz, 3)
+        y = np.zeros_like(u)
+        h = 1.0 / nx if h is None else float(h)
+        self._check(self.lib.femh_apply_operator(self.h, nx, ny, nz, h, _ptr(rho), _ptr(u), _ptr(y), 0))
+        self.shape = None
+        return y
+
+    def batch(self, rhos: Sequence[np.ndarray], h: float | None = None, dLdC=None, allow_unconverged=False):
+        """Many cells in one set of launches.  Returns (C [n,6,6], infos, dLdrho list or None)."""
+        n = len(rhos)
+        rhos = [np.ascontiguousarray(r, dtype=np.float64) for r in rhos]
+        cells = (_Cell * n)()
+        for i, r in enumerate(rhos):
+            cells[i].nx, cells[i].ny, cells[i].nz = r.shape
+            cells[i].h = (1.0 / r.shape[0]) if h is None else h
+            cells[i].rho = r.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        C = np.zeros((n, 6, 6))
+        infos = (_Info * n)()
+        g = None
+        gp = ctypes.c_void_p(0)
+        dp = ctypes.c_void_p(0)
+        if dLdC is not None:
+            dLdC = np.ascontiguousarray(dLdC, dtype=np.float64).reshape(n, 6, 6)
+            g = np.zeros(sum(r.size for r in rhos))
+            gp = _ptr(g)
+            dp = _ptr(dLdC)
+        st = self.lib.femh_homogenize_batch(self.h, n, cells, C.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                            dp, gp, infos)
+        allow = (FEMH_OK, FEMH_E_NOT_CONVERGED, FEMH_E_BREAKDOWN) if allow_unconverged else (FEMH_OK,)
+        self._check(st, allow)
+        grads = None
+        if g is not None:
+            grads, o = [], 0
+            for r in rhos:
+                grads.append(g[o:o + r.size].reshape(r.shape))
+                o += r.size
+        return C, [_info_dict(i) for i in infos], grads

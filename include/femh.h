@@ -1,0 +1,158 @@
+/*
+ * femh.h -- C ABI of the B200 voxel-FEM homogenization engine (libfemh.so).
+ *
+ * The engine computes the homogenized 6x6 elasticity tensor C^H of periodic
+ * voxel cells (trilinear hex8 elements, one shared element stiffness scaled
+ * per voxel), its density gradient, and batches of cells of uneven size, on
+ * one NVIDIA B200 (sm_100a).  It replaces the solve + energy reduction behind
+ * the reference's homogenization calls (desaic/fem):
+ *   - fast_fem FEM3DFun::setParam / f / df           (fast_fem/FEM3DFun.cpp:128-268,
+ *     RealFun virtuals fast_fem/RealFun.hpp:29-36), which drive topoOptLib's
+ *     Homogenization<3>::Homogenize() (fast_fem/FEM3DFun.cpp:153-154);
+ *   - NumericalCoarseningUsingMultigrid::computeCoarsenedElasticityTensorAndParameters3D
+ *     (SamplesGenerator/NumericalCoarseningUsingMultigrid.h:27-30,
+ *      SamplesGenerator/NumericalCoarseningUsingMultiGrid.cpp:221-345).
+ *
+ * Conventions
+ *   - voxel index (i*ny + j)*nz + k (x slowest, z fastest), the reference's
+ *     gridToLinearIdx / getGridToVectorIndex (Utilities/src/cfgMaterialUtilities.cpp:1003-1007);
+ *   - Voigt order xx, yy, zz, yz, xz, xy with engineering shear
+ *     (MaterialOpt/src/Homogenize3D.cpp:196-201, femlib/src/MeshUtilities.cpp:852-857);
+ *   - C_out is row-major 6x6 and symmetric (the reference fills only the
+ *     upper triangle of its G, fast_fem/FEM3DFun.cpp:163-178; both halves here);
+ *   - lower-triangle order of 21-entry outputs: (0,0),(1,0),(1,1),(2,0),...
+ *     (the order NumericalCoarseningUsingMultiGrid.cpp:315-324 appends);
+ *   - node 0 of every cell is pinned (removes the 3 translations); C^H does not
+ *     depend on that choice.
+ * Threading: one handle = one CUDA stream; calls on one handle are serialised
+ * by the caller; different handles are independent.
+ * Ownership: inputs and outputs belong to the caller; the handle keeps its own
+ * copies of the solved fields for the gradient calls.
+ * Errors: every function returns a femh_status; femh_last_error() gives text.
+ */
+#ifndef FEMH_H
+#define FEMH_H
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int femh_status;
+enum {
+  FEMH_OK = 0,
+  FEMH_E_ARG = 1,            /* invalid argument (sizes, pointers, config) */
+  FEMH_E_CUDA = 2,           /* CUDA runtime error */
+  FEMH_E_OOM = 3,            /* device allocation failed */
+  FEMH_E_NOT_CONVERGED = 4,  /* max_iter reached; results written, see info */
+  FEMH_E_BREAKDOWN = 5,      /* CG breakdown (p.Kp <= 0 or non-finite) */
+  FEMH_E_STATE = 6           /* call order (e.g. gradient before a solve) */
+};
+
+/* material law of the per-voxel Young's modulus E(rho); K0 uses nu */
+enum { FEMH_INTERP_SIMP = 0,    /* E_min + rho^p (E_s - E_min)   (BASELINE law) */
+       FEMH_INTERP_RAMP3 = 1,   /* E_s rho/(3-2rho)  fast_fem/FEM3DFun.cpp:20-27 */
+       FEMH_INTERP_BINARY = 2   /* rho>=0.5 ? bin_hi : bin_lo
+                                   NumericalCoarseningUsingMultiGrid.cpp:235-241 */ };
+enum { FEMH_FP64 = 0,           /* plain method, all FP64 */
+       FEMH_MIXED = 1 };        /* FP32 inner solve in FP64 defect correction */
+enum { FEMH_JACOBI_PCG = 0, FEMH_GMG_PCG = 1 };
+
+typedef struct {
+  int device;             /* CUDA device ordinal */
+  int interp;             /* FEMH_INTERP_* */
+  double E_s, E_min, penal, nu;
+  double bin_hi, bin_lo;
+  double rho_min, rho_max; /* clamp applied before the law (fast_fem clamps 1e-3..1) */
+  int precision;          /* FEMH_FP64 | FEMH_MIXED */
+  int solver;             /* FEMH_JACOBI_PCG | FEMH_GMG_PCG */
+  int pre_smooth, post_smooth; /* damped-Jacobi sweeps per level (GMG) */
+  double omega;           /* Jacobi damping */
+  int coarse_max_nodes;   /* coarsen until a level has <= this many nodes (GMG) */
+  double tol;             /* relative residual ||b - K x|| / ||b||, FP64 */
+  int max_iter;           /* CG iterations (plain) / inner iterations per outer step (mixed) */
+  double inner_tol;       /* mixed: relative reduction asked of each inner solve */
+  int max_outer;          /* mixed: defect-correction steps */
+  int store_bf16;         /* mixed: bf16 storage of search directions and rho */
+  int graph_chunk;        /* CG iterations per captured CUDA graph (0 = no graphs) */
+} femh_config;
+
+typedef struct {
+  int status;             /* FEMH_OK / FEMH_E_NOT_CONVERGED / FEMH_E_BREAKDOWN */
+  int iterations[6];      /* total inner CG iterations per load case */
+  int outer_iterations;   /* defect-correction steps (mixed), 1 for FP64 */
+  double rel_residual[6]; /* final FP64 ||b - K x|| / ||b|| per load case */
+  double solve_ms;        /* device time of the solve (CUDA events) */
+  double density;         /* mean rho used (fast_fem/FEM3DFun.cpp:189-193) */
+} femh_solve_info;
+
+typedef struct {
+  int nx, ny, nz;         /* voxels per axis (periodic) */
+  double h;               /* voxel edge; |Y| = nx*ny*nz*h^3 */
+  const double* rho;      /* nx*ny*nz densities (host or device, per call flag) */
+} femh_cell;
+
+typedef struct femh_handle femh_handle;
+
+/* Defaults: SIMP E_s=1, E_min=1e-6, p=3, nu=0.3, FP64 GMG-PCG, tol 1e-10. */
+femh_status femh_config_default(femh_config* cfg);
+
+/* Create an engine on cfg->device.  Replaces ElasticHexFEM/Homogenization
+ * initialisation (fast_fem/run3d.cpp:118-164,
+ * NumericalCoarseningUsingMultiGrid.cpp:134-218). */
+femh_status femh_create(femh_handle** h, const femh_config* cfg);
+femh_status femh_destroy(femh_handle* h);
+
+/* Solve the six periodic load cases of one cell and return C^H (6x6, row
+ * major).  rho has nx*ny*nz entries, on the device if rho_on_device.
+ * Replaces FEM3DFun::setParam's Homogenize + energy loop
+ * (fast_fem/FEM3DFun.cpp:128-196) and
+ * NumericalCoarseningUsingMultiGrid.cpp:269-313. */
+femh_status femh_homogenize(femh_handle* h, int nx, int ny, int nz, double hvox, const double* rho,
+                            int rho_on_device, double C_out[36], femh_solve_info* info);
+
+/* dL/drho_e for a loss with dL/dC = dLdC (6x6 row major) at the last solve:
+ * dL/drho_e = c'(rho_e) h/|Y| sum_IJ dLdC_IJ u^I_e.K0(1) u^J_e  (self-adjoint,
+ * no second solve).  Replaces FEM3DFun::df (fast_fem/FEM3DFun.cpp:222-268). */
+femh_status femh_homogenize_grad(femh_handle* h, const double dLdC[36], double* dLdrho,
+                                 int out_on_device);
+
+/* dC^H_IJ/drho_e for the 21 lower-triangle pairs, layout [21][nx*ny*nz]. */
+femh_status femh_dCdrho(femh_handle* h, double* out, int out_on_device);
+
+/* Full-cell displacement of load case I on (nx+1)(ny+1)(nz+1) nodes, layout
+ * [node][3] with node (i*(ny+1)+j)*(nz+1)+k, including the affine jump on the
+ * + faces: fast_fem/FEM3DFun.cpp:31-56 copyPeriodicU. */
+femh_status femh_full_field(femh_handle* h, int load_case, double* u_out, int out_on_device);
+
+/* Periodic fluctuation chi of the last solve, layout [6][nx*ny*nz][3]. */
+femh_status femh_fluctuation(femh_handle* h, double* chi_out, int out_on_device);
+
+/* Apply the periodic operator: y_I = K(rho) u_I for the 6 fields u, layout
+ * [6][nx*ny*nz][3] (the reference's assembled K, e.g.
+ * SamplesGenerator/NumericalCoarsening.cpp:1238-1306, matrix-free). */
+femh_status femh_apply_operator(femh_handle* h, int nx, int ny, int nz, double hvox,
+                                const double* rho, const double* u, double* y, int on_device);
+
+/* Many cells of uneven size in one set of launches (the sample generator's
+ * 8-thread loop, SamplesGenerator/SamplesGeneratorImpl.cpp:3703-3736).
+ * C_out: 36*ncell.  dLdC (36*ncell) and dLdrho (sum of voxels, cell after cell)
+ * are optional (both NULL to skip the gradient).  infos: ncell entries or NULL.
+ * All pointers host-side. */
+femh_status femh_homogenize_batch(femh_handle* h, int ncell, const femh_cell* cells, double* C_out,
+                                  const double* dLdC, double* dLdrho, femh_solve_info* infos);
+
+/* Copy the last error message (NUL-terminated) into buf. */
+femh_status femh_last_error(const femh_handle* h, char* buf, size_t n);
+
+/* Stream used by the handle (cudaStream_t as void*); NULL restores its own. */
+femh_status femh_set_stream(femh_handle* h, void* stream);
+
+/* Kernel launches issued by the handle since creation (all are this library's
+ * own kernels). */
+long long femh_kernel_launches(const femh_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FEMH_H */

@@ -1,0 +1,113 @@
+"""CPU checks of the FP64 oracle against the reference's golden fixture and
+closed-form known answers (pins the oracle before it is trusted as the
+checker of the GPU engine)."""
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "k0_lkh8_nu045.txt")
+# lk_H8 node a <-> z-fastest `oneV` node (fast_fem/FEM3DFun.cpp:58-60)
+LKH8_TO_ONEV = [0, 4, 6, 2, 1, 5, 7, 3]
+
+
+def _golden_k0():
+    return np.loadtxt(GOLDEN, comments="#")
+
+
+def test_k0_matches_reference_fixture(oracle):
+    """K0(E=1, nu=0.45, h=1) equals the reference's tests/1.K (lk_H8 order)."""
+    K = oracle.k0(1.0, 0.45, 1.0)
+    idx = [3 * LKH8_TO_ONEV[a] + c for a in range(8) for c in range(3)]
+    ref = _golden_k0()
+    assert np.abs(K[np.ix_(idx, idx)] - ref).max() < 1e-12
+
+
+def test_k0_properties(oracle):
+    for nu in (0.0, 0.3, 0.45):
+        K = oracle.k0(2.0, nu, 0.25)
+        assert np.abs(K - K.T).max() < 1e-14
+        # rigid translations are in the null space
+        for c in range(3):
+            t = np.zeros(24)
+            t[c::3] = 1
+            assert np.abs(K @ t).max() < 1e-13
+        w = np.linalg.eigvalsh(K)
+        assert (w > -1e-12).all() and (w > 1e-10).sum() == 18
+        # K0 scales with E * h in 3-D
+        assert np.allclose(oracle.k0(1.0, nu, 1.0) * 2.0 * 0.25, K, atol=1e-14)
+
+
+def test_uniform_cell_is_isotropic(oracle):
+    rho = np.ones((6, 6, 6))
+    C, chi, it, rel, st = oracle.homogenize(rho)
+    assert st == 0
+    assert np.abs(C - oracle.c_iso(1.0, 0.3)).max() < 1e-12
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_voxel_laminate_exact(oracle, axis):
+    """A layered cell's FE solution is piecewise linear across the layers and
+    is represented exactly by trilinear voxels: C^H = laminate formula."""
+    n = 8
+    prof = np.array([1.0, 0.3, 0.3, 1.0, 0.6, 0.2, 1.0, 0.9])
+    shape = [1, 1, 1]
+    shape[axis] = n
+    rho = np.broadcast_to(prof.reshape(shape), (n, n, n)).copy()
+    mat = oracle.material()
+    C, chi, it, rel, st = oracle.homogenize(rho, mat=mat)
+    Es = [oracle.lib().fo_coef(mat, float(r)) for r in prof]
+    Cref = oracle.c_laminate(Es, 0.3, axis)
+    assert np.abs(C - Cref).max() < 1e-9 * np.abs(Cref).max()
+
+
+def test_axis_permutation_equivariance(oracle):
+    rng = np.random.default_rng(3)
+    rho = (rng.random((6, 6, 6)) < 0.6).astype(float)
+    C, *_ = oracle.homogenize(rho)
+    # swap x and y: Voigt xx<->yy, yz<->xz
+    P = [1, 0, 2, 4, 3, 5]
+    C2, *_ = oracle.homogenize(np.ascontiguousarray(rho.transpose(1, 0, 2)))
+    assert np.abs(C2 - C[np.ix_(P, P)]).max() < 1e-8 * np.abs(C).max()
+    # periodic translation invariance
+    C3, *_ = oracle.homogenize(np.roll(rho, (2, 1, 3), axis=(0, 1, 2)))
+    assert np.abs(C3 - C).max() < 1e-8 * np.abs(C).max()
+
+
+def test_energy_gradient_vs_finite_differences(oracle):
+    """dL/drho of L = ||C - Ct||_F^2 from the adjoint formula against central
+    differences of the full solve (the reference's check_df pattern,
+    fast_fem/run3d.cpp:291-323)."""
+    rng = np.random.default_rng(4)
+    n = 4
+    rho = 0.3 + 0.6 * rng.random((n, n, n))
+    mat = oracle.material()
+    C, chi, *_ = oracle.homogenize(rho, mat=mat, tol=1e-13)
+    Ct = oracle.c_iso(0.2, 0.3)
+    dLdC = 2 * (C - Ct)
+    g = oracle.grad(rho, chi, dLdC, mat=mat)
+    hstep = 1e-6
+    for flat in rng.choice(n ** 3, 5, replace=False):
+        i = np.unravel_index(flat, rho.shape)
+        rp = rho.copy(); rp[i] += hstep
+        rm = rho.copy(); rm[i] -= hstep
+        Lp = np.sum((oracle.homogenize(rp, mat=mat, tol=1e-13)[0] - Ct) ** 2)
+        Lm = np.sum((oracle.homogenize(rm, mat=mat, tol=1e-13)[0] - Ct) ** 2)
+        fd = (Lp - Lm) / (2 * hstep)
+        assert abs(fd - g[i]) <= 1e-5 * max(abs(fd), 1e-3 * np.abs(g).max())
+
+
+def test_dCdrho_consistent_with_grad(oracle):
+    rng = np.random.default_rng(5)
+    rho = 0.2 + 0.7 * rng.random((4, 4, 4))
+    C, chi, *_ = oracle.homogenize(rho)
+    d = oracle.dCdrho(rho, chi)
+    W = rng.standard_normal((6, 6))
+    g = oracle.grad(rho, chi, W)
+    t = 0
+    acc = np.zeros_like(rho)
+    for I in range(6):
+        for J in range(I + 1):
+            acc += d[t] * (W[I, I] if I == J else W[I, J] + W[J, I])
+            t += 1
+    assert np.abs(acc - g).max() < 1e-12 * np.abs(g).max()
