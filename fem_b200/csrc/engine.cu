@@ -249,7 +249,7 @@ struct femh_handle {
 
   // setup cache
   std::vector<int> shape_key;
-  double h_key = -1;
+  std::vector<double> h_key;
   int prec_key = -1, solver_key = -1;
   Arena setup;
   std::vector<Level> levels;
@@ -394,11 +394,11 @@ inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) /
 // ====================================================== setup / solve ===
 namespace {
 
-void build_setup(femh_handle* H, const std::vector<int>& shapes, double h) {
+void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vector<double>& hs) {
   const femh_config& c = H->cfg;
   const bool mixed = c.precision == FEMH_MIXED;
   const bool gmg = c.solver == FEMH_GMG_PCG;
-  if (H->shape_key == shapes && H->h_key == h && H->prec_key == c.precision && H->solver_key == c.solver)
+  if (H->shape_key == shapes && H->h_key == hs && H->prec_key == c.precision && H->solver_key == c.solver)
     return;
   H->setup.release();
   H->levels.clear();
@@ -413,7 +413,8 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, double h) {
   for (int i = 0; i < nc; ++i) {
     const int nx = shapes[3 * i], ny = shapes[3 * i + 1], nz = shapes[3 * i + 2];
     if (nx < 2 || ny < 2 || nz < 2) throw FemhError{FEMH_E_ARG, "each cell needs >= 2 voxels per axis"};
-    if (nz > 512) throw FemhError{FEMH_E_ARG, "nz > 512 is not supported"};
+    if (nz > 256) throw FemhError{FEMH_E_ARG, "nz > 256 is not supported"};
+    if (!(hs[i] > 0.0)) throw FemhError{FEMH_E_ARG, "voxel edge h must be positive"};
     H->cell_vox[i] = (long long)nx * ny * nz;
     H->cell_off[i] = off;
     off += H->cell_vox[i];
@@ -454,7 +455,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, double h) {
       cd.parent = l > 0 ? idx_at[l - 1][i] : -1;
       cd.child = -1;
       cd.off = loff;
-      cd.h = h * (double)(1 << l);
+      cd.h = hs[i] * (double)(1 << l);
       idx_at[l][i] = (int)L.cells.size();
       L.cells.push_back(cd);
       loff += (long long)cd.nx * cd.ny * cd.nz;
@@ -546,7 +547,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, double h) {
   H->d_out = ar.arr<double>(21 * nv);
   H->d_nrm = ar.arr<double>(nc * kNumRhs);
   H->shape_key = shapes;
-  H->h_key = h;
+  H->h_key = hs;
   H->prec_key = c.precision;
   H->solver_key = c.solver;
 }
@@ -907,10 +908,10 @@ void energy_C(femh_handle* H, std::vector<double>& C, std::vector<double>& dens)
 }
 
 // Common path of single-cell and batched calls.  rho_ptrs[i] host or device.
-void run_cells(femh_handle* H, const std::vector<int>& shapes, double h, const std::vector<const double*>& rho,
-               bool rho_dev, std::vector<double>& C, std::vector<femh_solve_info>& infos) {
-  if (!(h > 0.0)) throw FemhError{FEMH_E_ARG, "voxel edge h must be positive"};
-  build_setup(H, shapes, h);
+void run_cells(femh_handle* H, const std::vector<int>& shapes, const std::vector<double>& hs,
+               const std::vector<const double*>& rho, bool rho_dev, std::vector<double>& C,
+               std::vector<femh_solve_info>& infos) {
+  build_setup(H, shapes, hs);
   cudaStream_t s = H->stream;
   for (int i = 0; i < H->ncells; ++i) {
     if (!rho[i]) throw FemhError{FEMH_E_ARG, "null rho"};
@@ -987,7 +988,7 @@ femh_status femh_config_default(femh_config* c) {
   c->solver = FEMH_GMG_PCG;
   c->pre_smooth = 2;
   c->post_smooth = 2;
-  c->omega = 0.6;
+  c->omega = 0.4;
   c->coarse_max_nodes = 64;
   c->tol = 1e-10;
   c->max_iter = 20000;
@@ -1050,7 +1051,7 @@ femh_status femh_homogenize(femh_handle* H, int nx, int ny, int nz, double hvox,
     CK(cudaSetDevice(H->device));
     std::vector<double> C;
     std::vector<femh_solve_info> infos;
-    run_cells(H, {nx, ny, nz}, hvox, {rho}, rho_on_device != 0, C, infos);
+    run_cells(H, {nx, ny, nz}, {hvox}, {rho}, rho_on_device != 0, C, infos);
     std::memcpy(C_out, C.data(), sizeof(double) * 36);
     if (info) *info = infos[0];
     code = infos[0].status;
@@ -1068,20 +1069,16 @@ femh_status femh_homogenize_batch(femh_handle* H, int ncell, const femh_cell* ce
     if ((dLdC == nullptr) != (dLdrho == nullptr)) throw FemhError{FEMH_E_ARG, "dLdC and dLdrho go together"};
     CK(cudaSetDevice(H->device));
     std::vector<int> shapes;
+    std::vector<double> hs;
     std::vector<const double*> rho;
-    const double h = cells[0].h;
     for (int i = 0; i < ncell; ++i) {
-      if (std::fabs(cells[i].h - h) > 1e-15 * h) {
-        // cells of different voxel size: run them one h-group at a time is not needed by the
-        // sample generator (unit cell, h = 1/n); per-cell h is folded into CellDesc below.
-      }
       shapes.insert(shapes.end(), {cells[i].nx, cells[i].ny, cells[i].nz});
+      hs.push_back(cells[i].h);
       rho.push_back(cells[i].rho);
     }
     std::vector<double> C;
     std::vector<femh_solve_info> infos;
-    // per-cell h: each cell's edge is 1/nx of its own unit cell when h <= 0 is given
-    run_cells(H, shapes, h, rho, false, C, infos);
+    run_cells(H, shapes, hs, rho, false, C, infos);
     std::memcpy(C_out, C.data(), sizeof(double) * 36 * ncell);
     if (infos_out) std::memcpy(infos_out, infos.data(), sizeof(femh_solve_info) * ncell);
     for (auto& I : infos)
@@ -1206,9 +1203,8 @@ femh_status femh_apply_operator(femh_handle* H, int nx, int ny, int nz, double h
   if (!H) return FEMH_E_ARG;
   return guard(H, [&] {
     if (!rho || !u || !y) throw FemhError{FEMH_E_ARG, "rho, u and y must not be NULL"};
-    if (!(hvox > 0.0)) throw FemhError{FEMH_E_ARG, "voxel edge h must be positive"};
     CK(cudaSetDevice(H->device));
-    build_setup(H, {nx, ny, nz}, hvox);
+    build_setup(H, {nx, ny, nz}, {hvox});
     cudaStream_t s = H->stream;
     const long long nn = H->nvox;
     const cudaMemcpyKind k_in = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;

@@ -660,7 +660,7 @@ __global__ void k_dc_accum(const CellDesc* cells, const NodeUnit* units, double*
   const int rhs = blockIdx.y;
   const CellDesc cd = cells[u.cell];
   const CGState S = stt[cd.id * kNumRhs + rhs];
-  if (!S.active) return;
+  if (!S.outer) return;
   const double inv = 1.0 / S.scale;
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x)
 #pragma unroll

@@ -115,7 +115,7 @@ class Config:
     solver: int = GMG_PCG
     pre_smooth: int = 2
     post_smooth: int = 2
-    omega: float = 0.6
+    omega: float = 0.4
     coarse_max_nodes: int = 64
     tol: float = 1e-10
     max_iter: int = 20000

@@ -1,0 +1,138 @@
+"""GPU parity of the CUDA engine (through the C ABI) against the FP64 oracle.
+
+Bars (written here):
+  * operator apply, FP64:                 1e-13 relative (max-norm)
+  * C^H, plain FP64 (Jacobi / GMG PCG):   1e-8 relative (max entry / max |C|)
+  * C^H, mixed precision (FP32 inner):    1e-6 relative
+  * gradients dL/drho, dC/drho:           1e-5 relative
+Sizes are the ones the oracle finishes in seconds; full-size cases are covered
+by size-independent properties in test_gpu_properties.py.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_APPLY = 1e-13
+TOL_FP64 = 1e-8
+TOL_MIXED = 1e-6
+TOL_GRAD = 1e-5
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.fixture(scope="module")
+def rng():
+    return np.random.default_rng(11)
+
+
+@pytest.mark.parametrize("shape", [(8, 8, 8), (6, 10, 4), (16, 16, 16), (12, 8, 20)])
+def test_apply_matches_oracle(femh, oracle, rng, shape):
+    rho = rng.random(shape)
+    u = rng.standard_normal((6,) + shape + (3,))
+    e = femh.Engine()
+    y = e.apply_operator(rho, u)
+    mat = oracle.material()
+    yo = oracle.apply(shape, oracle.k0(1.0, 0.3, 1.0 / shape[0]), oracle.coef(mat, rho), u)
+    assert _rel(y, yo) < TOL_APPLY
+
+
+def test_apply_deterministic(femh, rng):
+    rho = rng.random((16, 16, 16))
+    u = rng.standard_normal((6, 16, 16, 16, 3))
+    e = femh.Engine()
+    assert np.array_equal(e.apply_operator(rho, u), e.apply_operator(rho, u))
+
+
+@pytest.mark.parametrize("solver", ["jacobi", "gmg"])
+@pytest.mark.parametrize("n", [8, 16, 32])
+def test_fp64_C_matches_oracle(femh, oracle, n, solver):
+    """The 32^3 binary cell (p = 0.5, seed 1) is the CPU parity workload."""
+    from fem_b200 import fields
+    rho = fields.binary_cell(n, 0.5, seed=1)
+    Co, *_ = oracle.homogenize(rho)
+    e = femh.Engine(solver=femh.JACOBI_PCG if solver == "jacobi" else femh.GMG_PCG)
+    C, info = e.homogenize(rho)
+    assert info["status"] == 0 and max(info["rel_residual"]) < 1e-10
+    assert _rel(C, Co) < TOL_FP64
+
+
+@pytest.mark.parametrize("solver", ["jacobi", "gmg"])
+@pytest.mark.parametrize("bf16", [0, 1])
+def test_mixed_C_matches_oracle(femh, oracle, solver, bf16):
+    from fem_b200 import fields
+    rho = fields.smooth_cell(16, sigma=2.0, seed=2)
+    Co, *_ = oracle.homogenize(rho)
+    e = femh.Engine(precision=femh.MIXED, store_bf16=bf16,
+                    solver=femh.JACOBI_PCG if solver == "jacobi" else femh.GMG_PCG)
+    C, info = e.homogenize(rho)
+    assert info["status"] == 0 and max(info["rel_residual"]) < 1e-10
+    assert _rel(C, Co) < TOL_MIXED
+
+
+@pytest.mark.parametrize("interp", ["simp", "ramp3", "binary"])
+def test_material_laws(femh, oracle, interp):
+    from fem_b200 import fields
+    rho = fields.smooth_cell(8, sigma=1.5, seed=5)
+    kw = {"simp": dict(interp=0), "ramp3": dict(interp=1, rho_min=1e-3),
+          "binary": dict(interp=2, bin_hi=1.0, bin_lo=1e-4)}[interp]
+    mat = oracle.material(interp=kw["interp"])
+    rho_o = np.clip(rho, kw.get("rho_min", 0.0), 1.0)
+    Co, *_ = oracle.homogenize(rho_o, mat=mat)
+    e = femh.Engine(**kw)
+    C, _ = e.homogenize(rho)
+    assert _rel(C, Co) < TOL_FP64
+
+
+def test_gradient_matches_oracle(femh, oracle):
+    from fem_b200 import fields
+    rho = fields.smooth_cell(12, sigma=2.0, seed=4)
+    Co, chi_o, *_ = oracle.homogenize(rho, tol=1e-12)
+    Ct = oracle.c_iso(0.05, 0.3)
+    dLdC = 2 * (Co - Ct)
+    go = oracle.grad(rho, chi_o, dLdC)
+    e = femh.Engine(tol=1e-12)
+    C, _ = e.homogenize(rho)
+    g = e.grad(2 * (C - Ct))
+    assert _rel(g, go) < TOL_GRAD
+    d = e.dCdrho()
+    do = oracle.dCdrho(rho, chi_o)
+    assert _rel(d, do) < TOL_GRAD
+
+
+def test_fluctuation_and_full_field(femh, oracle):
+    """chi matches the oracle's (same pinned node), and the full-cell field is
+    copyPeriodicU's: periodic chi plus eps.X with the jump on the + faces."""
+    from fem_b200 import fields
+    n = 8
+    rho = fields.binary_cell(n, 0.6, seed=9)
+    Co, chi_o, *_ = oracle.homogenize(rho, tol=1e-12)
+    e = femh.Engine(tol=1e-12)
+    e.homogenize(rho)
+    chi = e.fluctuation()
+    assert np.abs(chi - chi_o).max() < 1e-7 * np.abs(chi_o).max()
+    h = 1.0 / n
+    for I in range(6):
+        u = e.full_field(I)
+        eps = np.zeros((3, 3))
+        if I < 3:
+            eps[I, I] = 1
+        else:
+            a, b = [(1, 2), (0, 2), (0, 1)][I - 3]
+            eps[a, b] = eps[b, a] = 0.5
+        X = np.stack(np.meshgrid(*(np.arange(n + 1) * h,) * 3, indexing="ij"), -1)
+        idx = np.arange(n + 1) % n
+        ref = chi[I][np.ix_(idx, idx, idx)] + X @ eps.T
+        assert np.abs(u - ref).max() < 1e-12
+
+
+def test_batch_matches_single(femh):
+    from fem_b200 import fields
+    rhos = [fields.binary_cell(n, 0.4, seed=20 + n) for n in (8, 12, 16, 8, 24)]
+    e = femh.Engine()
+    Cb, infos, _ = e.batch(rhos, h=None)
+    for r, C in zip(rhos, Cb):
+        Cs, _ = femh.Engine().homogenize(r)
+        assert _rel(C, Cs) < TOL_FP64
