@@ -14,8 +14,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfemh.so")
-SOURCES = ["engine.cu"]
-HEADERS = ["femh_common.cuh", "stencil.cuh", "kernels.cuh"]
+SOURCES = [os.path.join(CSRC, "engine.cu"), os.path.join(HERE, "host", "femh_host.cpp")]
+HEADERS = [os.path.join(CSRC, f) for f in ("femh_common.cuh", "stencil.cuh", "kernels.cuh")] + [
+    os.path.join(HERE, "host", "femh_host.hpp")]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 FLAGS = [
@@ -32,14 +33,14 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "femh.h")]
+    deps = SOURCES + HEADERS + [os.path.join(ROOT, "include", "femh.h"), os.path.abspath(__file__)]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
 def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> str:
     if not force and not _stale():
         return LIB
-    cmd = [NVCC, *FLAGS, "-o", LIB, *[os.path.join(CSRC, s) for s in SOURCES], "-lcudart"]
+    cmd = [NVCC, *FLAGS, "-o", LIB, *SOURCES, "-lcudart"]
     if ptxas_v:
         cmd.insert(1, "-Xptxas=-v")
     if verbose:

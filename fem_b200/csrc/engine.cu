@@ -8,8 +8,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -206,7 +208,8 @@ struct UnitList {
 struct Level {
   std::vector<CellDesc> cells;
   CellDesc* d_cells = nullptr;
-  long long ntot = 0;
+  long long ntot = 0, nodes_smooth = 0;
+  int level = 0;
   int NT = 256, maxnz = 1;
   UnitList all, smooth;      // all cells / cells that continue to a coarser level
   std::vector<int> su_sb, su_se, nu_sb, nu_se;   // slot ranges per cell (all lists)
@@ -282,9 +285,82 @@ struct femh_handle {
   std::vector<double> C_last;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  // measurement: per-kernel-class CUDA-event timing (femh_profile), and the
+  // count of kernel executions including CUDA-graph replays
+  bool prof = false;
+  bool capturing = false;
+  long long cap_count = 0;
+  struct KStat {
+    long long launches = 0;
+    double ms = 0, bytes = 0;
+  };
+  std::map<std::string, KStat> kstats;
+  struct Pend {
+    std::string name;
+    cudaEvent_t a, b;
+    double bytes;
+  };
+  std::vector<Pend> pend;
+  std::vector<cudaEvent_t> evpool;
 };
 
 namespace {
+
+#define LAUNCH_CHECK(H)                          \
+  do {                                           \
+    CK(cudaGetLastError());                      \
+    if ((H)->capturing) (H)->cap_count++;        \
+    else (H)->launches++;                        \
+  } while (0)
+
+cudaEvent_t pool_event(femh_handle* H) {
+  if (!H->evpool.empty()) {
+    cudaEvent_t e = H->evpool.back();
+    H->evpool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  CK(cudaEventCreate(&e));
+  return e;
+}
+
+// Times the launches issued in its scope when profiling is on (graphs are
+// not captured then, so every launch is timed on the handle's stream).
+struct Prof {
+  femh_handle* H;
+  const char* name;
+  double bytes;
+  cudaEvent_t a = nullptr;
+  Prof(femh_handle* h, const char* n, double b) : H(h), name(n), bytes(b) {
+    if (H->prof && !H->capturing) {
+      a = pool_event(H);
+      CK(cudaEventRecord(a, H->stream));
+    }
+  }
+  ~Prof() {
+    if (a) {
+      cudaEvent_t b = pool_event(H);
+      if (cudaEventRecord(b, H->stream) == cudaSuccess) H->pend.push_back({name, a, b, bytes});
+    }
+  }
+};
+
+void prof_resolve(femh_handle* H) {
+  if (H->pend.empty()) return;
+  CK(cudaStreamSynchronize(H->stream));
+  for (auto& p : H->pend) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, p.a, p.b));
+    auto& k = H->kstats[p.name];
+    k.launches++;
+    k.ms += ms;
+    k.bytes += p.bytes;
+    H->evpool.push_back(p.a);
+    H->evpool.push_back(p.b);
+  }
+  H->pend.clear();
+}
 
 void set_err(femh_handle* h, const std::string& m) {
   if (h) h->err = m;
@@ -326,7 +402,7 @@ void add_stencil_units(std::vector<StencilUnit>& out, int cellidx, const CellDes
 }
 
 void add_node_units(std::vector<NodeUnit>& out, int cellidx, long long nn, int& slot) {
-  const long long chunk = 4096;
+  const long long chunk = 2048;
   for (long long b = 0; b < nn; b += chunk)
     out.push_back(NodeUnit{cellidx, slot++, b, std::min(nn, b + chunk)});
 }
@@ -347,8 +423,7 @@ void stencil_go(femh_handle* H, dim3 grid, size_t smem, const StencilArgs<TIn, T
     attr = true;
   }
   fn<<<grid, NT, smem, H->stream>>>(a);
-  CK(cudaGetLastError());
-  H->launches++;
+  LAUNCH_CHECK(H);
 }
 
 // T = arithmetic type; in/out/b storage types as given.
@@ -372,6 +447,14 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   a.omega = omega;
   const size_t smem = sizeof(T) * (size_t)(15 * L.NT + 3 * L.maxnz) + 64 * sizeof(double);
   dim3 grid((unsigned)ul.su.size(), kNumRhs);
+  static const char* mode_names[] = {"apply", "apply_dot", "jacobi", "jacobi_dot", "resid"};
+  char nm[64];
+  snprintf(nm, sizeof nm, "stencil_%s_%s_L%d", sizeof(T) == 8 ? "f64" : "f32", mode_names[OUT], L.level);
+  const double nodes = (double)(smooth_only ? L.nodes_smooth : L.ntot);
+  double per = 18.0 * (sizeof(TIn) + sizeof(TOut)) + sizeof(TC);
+  if (OUT >= OUT_JACOBI) per += 18.0 * sizeof(TB) + (OUT == OUT_RESID ? 0.0 : 4.0);
+  std::string key(nm);
+  Prof prof_(H, H->prof ? H->kstats.emplace(key, femh_handle::KStat{}).first->first.c_str() : nm, nodes * per);
   switch (L.NT) {
     case 128: stencil_go<T, 128, OUT>(H, grid, smem, a); break;
     case 256: stencil_go<T, 256, OUT>(H, grid, smem, a); break;
@@ -381,11 +464,7 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
 }
 
 #define NODE_GRID(ul) dim3((unsigned)(ul).nu.size(), kNumRhs)
-#define LAUNCH_CHECK(H) \
-  do {                  \
-    CK(cudaGetLastError()); \
-    (H)->launches++;    \
-  } while (0)
+
 
 inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
@@ -482,6 +561,9 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
       add_node_units(L.all.nu, ci, (long long)cd.nx * cd.ny * cd.nz, sn);
       L.nu_se.push_back(sn);
     }
+    L.level = l;
+    for (auto& cd : L.cells)
+      if (cd.child >= 0) L.nodes_smooth += (long long)cd.nx * cd.ny * cd.nz;
     for (auto& u : L.all.su)
       if (L.cells[u.cell].child >= 0) L.smooth.su.push_back(u);
     for (auto& u : L.all.nu)
@@ -559,39 +641,65 @@ void prepare_operator(femh_handle* H) {
   cudaStream_t s = H->stream;
   Level& L0 = H->levels[0];
   const MatLaw law = make_law(c);
-  k_coef<TC><<<(unsigned)L0.all.nu.size(), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->rho_in, law, H->kc64,
+  {
+    Prof prof_(H, "k_coef", 0.0);
+    k_coef<TC><<<(unsigned)L0.all.nu.size(), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->rho_in, law, H->kc64,
                                                         std::is_same<TC, double>::value ? nullptr : (TC*)L0.kc,
                                                         H->rho_used);
-  LAUNCH_CHECK(H);
+    LAUNCH_CHECK(H);
+  }
   if (std::is_same<TC, double>::value)
     CK(cudaMemcpyAsync(L0.kc, H->kc64, sizeof(double) * H->nvox, cudaMemcpyDeviceToDevice, s));
   for (size_t l = 1; l < H->levels.size(); ++l) {
     Level& L = H->levels[l];
     Level& F = H->levels[l - 1];
-    k_coarsen_coef<TC, TC><<<(unsigned)L.all.nu.size(), 256, 0, s>>>(F.d_cells, L.d_cells, L.all.d_nu,
+    {
+      Prof prof_(H, "k_coarsen_coef", 0.0);
+      k_coarsen_coef<TC, TC><<<(unsigned)L.all.nu.size(), 256, 0, s>>>(F.d_cells, L.d_cells, L.all.d_nu,
                                                                      (const TC*)F.kc, (TC*)L.kc);
-    LAUNCH_CHECK(H);
-  }
-  for (auto& L : H->levels) {
-    k_invdiag<TC><<<(unsigned)L.all.nu.size(), 256, 0, s>>>(L.d_cells, L.all.d_nu, (const TC*)L.kc,
-                                                            H->hk.diag, L.invd);
-    LAUNCH_CHECK(H);
-    if (!L.coarse_list.empty()) {
-      const unsigned n = (unsigned)L.coarse_list.size();
-      k_coarse_assemble<TC><<<n, 256, 0, s>>>(L.d_cells, L.d_coarse_list, (const TC*)L.kc, H->d_K0, L.d_A,
-                                              L.d_aoff);
-      LAUNCH_CHECK(H);
-      k_coarse_factor<<<n, 256, 0, s>>>(L.d_cells, L.d_coarse_list, L.d_A, L.d_Awork, L.d_aoff, L.d_cstat);
       LAUNCH_CHECK(H);
     }
   }
+  for (auto& L : H->levels) {
+    {
+      Prof prof_(H, "k_invdiag", 0.0);
+      k_invdiag<TC><<<(unsigned)L.all.nu.size(), 256, 0, s>>>(L.d_cells, L.all.d_nu, (const TC*)L.kc,
+                                                            H->hk.diag, L.invd);
+      LAUNCH_CHECK(H);
+    }
+    if (!L.coarse_list.empty()) {
+      const unsigned n = (unsigned)L.coarse_list.size();
+      {
+        Prof prof_(H, "k_coarse_assemble", 0.0);
+        k_coarse_assemble<TC><<<n, 256, 0, s>>>(L.d_cells, L.d_coarse_list, (const TC*)L.kc, H->d_K0, L.d_A,
+                                              L.d_aoff);
+        LAUNCH_CHECK(H);
+      }
+      {
+        Prof prof_(H, "k_coarse_factor", 0.0);
+        k_coarse_factor<<<n, 256, 0, s>>>(L.d_cells, L.d_coarse_list, L.d_A, L.d_Awork, L.d_aoff, L.d_cstat);
+        LAUNCH_CHECK(H);
+      }
+    }
+  }
   // loads
-  k_rhs<double><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->kc64, H->d_ec, H->b64, L0.ntot);
-  LAUNCH_CHECK(H);
+  {
+    Prof prof_(H, "k_rhs", 0.0);
+    k_rhs<double><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->kc64, H->d_ec, H->b64, L0.ntot);
+    LAUNCH_CHECK(H);
+  }
 }
 
 
-unsigned fin_blocks(int nc) { return cdiv((long long)nc * kNumRhs, 128); }
+bool verbose() {
+  static const int v = [] {
+    const char* e = std::getenv("FEMH_VERBOSE");
+    return (e && *e && *e != '0') ? 1 : 0;
+  }();
+  return v != 0;
+}
+
+unsigned fin_blocks(int nc) { return cdiv((long long)nc * kNumRhs * 32, 128); }   // a warp per (cell, rhs)
 
 // One V-cycle of the multigrid preconditioner: z = V(r0).  Level 0's xa must
 // already hold the first damped-Jacobi sweep omega*invd*r0 (written by the CG
@@ -619,17 +727,23 @@ TV* vcycle(femh_handle* H, const TV* r0) {
     const TV* b = (l == 0) ? r0 : (const TV*)L.bv;
     if (!L.coarse_list.empty()) {
       dim3 g((unsigned)L.coarse_list.size(), kNumRhs);
-      k_coarse_solve<TV, TV><<<g, 256, sizeof(double) * L.coarse_maxm, s>>>(
+      {
+        Prof prof_(H, "k_coarse_solve", 0.0);
+        k_coarse_solve<TV, TV><<<g, 256, sizeof(double) * L.coarse_maxm, s>>>(
           L.d_cells, L.d_coarse_list, L.d_A, L.d_aoff, b, sol[l], stt, L.ntot);
-      LAUNCH_CHECK(H);
+        LAUNCH_CHECK(H);
+      }
     }
     if (L.smooth.su.empty()) continue;
     TV* cur = (TV*)L.xa;
     TV* oth = (TV*)L.xb;
     if (l > 0) {
-      k_jacobi0<TV, TV><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, L.smooth.d_nu, b, cur, L.invd, om,
+      {
+        Prof prof_(H, "k_jacobi0", 0.0);
+        k_jacobi0<TV, TV><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, L.smooth.d_nu, b, cur, L.invd, om,
                                                             stt, L.ntot);
-      LAUNCH_CHECK(H);
+        LAUNCH_CHECK(H);
+      }
     }
     for (int sw = 1; sw < c.pre_smooth; ++sw) {
       stencil<TV, OUT_JACOBI>(H, L, true, (const TV*)cur, oth, b, (const TC*)L.kc, nullptr, stt, om);
@@ -637,9 +751,12 @@ TV* vcycle(femh_handle* H, const TV* r0) {
     }
     stencil<TV, OUT_RESID>(H, L, true, (const TV*)cur, oth, b, (const TC*)L.kc, nullptr, stt, om);
     Level& C = H->levels[l + 1];
-    k_restrict<TV, TV><<<NODE_GRID(C.all), 256, 0, s>>>(L.d_cells, C.d_cells, C.all.d_nu, oth, (TV*)C.bv, stt,
+    {
+      Prof prof_(H, "k_restrict", 0.0);
+      k_restrict<TV, TV><<<NODE_GRID(C.all), 256, 0, s>>>(L.d_cells, C.d_cells, C.all.d_nu, oth, (TV*)C.bv, stt,
                                                         L.ntot, C.ntot);
-    LAUNCH_CHECK(H);
+      LAUNCH_CHECK(H);
+    }
   }
   for (int l = nlev - 2; l >= 0; --l) {
     Level& L = H->levels[l];
@@ -648,9 +765,12 @@ TV* vcycle(femh_handle* H, const TV* r0) {
     const TV* b = (l == 0) ? r0 : (const TV*)L.bv;
     TV* x = sm[l];
     TV* t = tmp[l];
-    k_prolong_add<TV, TV><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, C.d_cells, L.smooth.d_nu, x,
+    {
+      Prof prof_(H, "k_prolong_add", 0.0);
+      k_prolong_add<TV, TV><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, C.d_cells, L.smooth.d_nu, x,
                                                               (const TV*)sol[l + 1], stt, L.ntot, C.ntot);
-    LAUNCH_CHECK(H);
+      LAUNCH_CHECK(H);
+    }
     for (int sw = 0; sw < c.post_smooth; ++sw) {
       stencil<TV, OUT_JACOBI>(H, L, true, (const TV*)x, t, b, (const TC*)L.kc, nullptr, stt, om);
       std::swap(x, t);
@@ -674,24 +794,39 @@ void pcg_iteration(femh_handle* H) {
   CGState* stt = H->d_state;
   stencil<TV, OUT_APPLY_DOT>(H, L0, false, (const TP*)p, q, (const TV*)nullptr, (const TC*)L0.kc, H->d_part_s,
                              stt, 0.0);
-  k_fin_alpha<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_su_sb, L0.d_su_se, H->d_part_s, nc);
-  LAUNCH_CHECK(H);
-  k_cg_update<TV, TP, TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(
+  {
+    Prof prof_(H, "k_fin_alpha", 0.0);
+    k_fin_alpha<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_su_sb, L0.d_su_se, H->d_part_s, nc);
+    LAUNCH_CHECK(H);
+  }
+  {
+    Prof prof_(H, "k_cg_update", 0.0);
+    k_cg_update<TV, TP, TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(
       L0.d_cells, L0.all.d_nu, x, r, p, q, L0.invd, gmg ? (TV*)L0.xa : (TV*)nullptr, c.omega, stt, H->d_part_n,
       L0.ntot);
-  LAUNCH_CHECK(H);
+    LAUNCH_CHECK(H);
+  }
   TV* z = nullptr;
   if (gmg) {
     z = vcycle<TV, TC>(H, r);
-    k_dot<TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
+    {
+      Prof prof_(H, "k_dot", 0.0);
+      k_dot<TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
+      LAUNCH_CHECK(H);
+    }
+  }
+  {
+    Prof prof_(H, "k_fin_beta", 0.0);
+    k_fin_beta<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_n, H->d_part_z, nc,
+                                            gmg ? 0 : 1);
     LAUNCH_CHECK(H);
   }
-  k_fin_beta<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_n, H->d_part_z, nc,
-                                            gmg ? 0 : 1);
-  LAUNCH_CHECK(H);
-  k_cg_dir<TP, TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, p, (const TV*)z,
+  {
+    Prof prof_(H, "k_cg_dir", 0.0);
+    k_cg_dir<TP, TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, p, (const TV*)z,
                                                          (const TV*)r, L0.invd, stt, L0.ntot);
-  LAUNCH_CHECK(H);
+    LAUNCH_CHECK(H);
+  }
 }
 
 // PCG on K x = scale*b for every (cell, rhs) whose state is active.
@@ -712,35 +847,59 @@ void pcg(femh_handle* H, const TB* b, int max_iter, double tol, int iters_out[])
     S.iters = 0;
   }
   CK(cudaMemcpyAsync(stt, H->state.data(), sizeof(CGState) * H->state.size(), cudaMemcpyHostToDevice, s));
-  k_cg_init<TB, TV, TP><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, b, x, r, p, L0.invd, stt,
+  {
+    Prof prof_(H, "k_cg_init", 0.0);
+    k_cg_init<TB, TV, TP><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, b, x, r, p, L0.invd, stt,
                                                           H->d_part_n, L0.ntot, gmg ? 0 : 1);
-  LAUNCH_CHECK(H);
-  k_fin_init<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_n, nc, gmg ? 0 : 1);
-  LAUNCH_CHECK(H);
+    LAUNCH_CHECK(H);
+  }
+  {
+    Prof prof_(H, "k_fin_init", 0.0);
+    k_fin_init<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_n, nc, gmg ? 0 : 1);
+    LAUNCH_CHECK(H);
+  }
   if (gmg) {
-    k_jacobi0<TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, r, (TV*)L0.xa, L0.invd,
+    {
+      Prof prof_(H, "k_jacobi0", 0.0);
+      k_jacobi0<TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, r, (TV*)L0.xa, L0.invd,
                                                         c.omega, stt, L0.ntot);
-    LAUNCH_CHECK(H);
+      LAUNCH_CHECK(H);
+    }
     TV* z = vcycle<TV, TC>(H, r);
-    k_copy<TP, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, p, z, stt, L0.ntot);
-    LAUNCH_CHECK(H);
-    k_dot<TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
-    LAUNCH_CHECK(H);
-    k_fin_rz<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_z, nc);
-    LAUNCH_CHECK(H);
+    {
+      Prof prof_(H, "k_copy", 0.0);
+      k_copy<TP, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, p, z, stt, L0.ntot);
+      LAUNCH_CHECK(H);
+    }
+    {
+      Prof prof_(H, "k_dot", 0.0);
+      k_dot<TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
+      LAUNCH_CHECK(H);
+    }
+    {
+      Prof prof_(H, "k_fin_rz", 0.0);
+      k_fin_rz<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_z, nc);
+      LAUNCH_CHECK(H);
+    }
   }
   const int chunk = std::max(1, c.graph_chunk > 0 ? c.graph_chunk : 8);
   cudaGraphExec_t exec = nullptr;
-  if (c.graph_chunk > 0) {
+  long long graph_kernels = 0;
+  if (c.graph_chunk > 0 && !H->prof) {
     cudaGraph_t g = nullptr;
+    H->capturing = true;
+    H->cap_count = 0;
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
       for (int i = 0; i < chunk; ++i) pcg_iteration<TV, TP, TC>(H);
     } catch (...) {
+      H->capturing = false;
       cudaStreamEndCapture(s, &g);
       if (g) cudaGraphDestroy(g);
       throw;
     }
+    H->capturing = false;
+    graph_kernels = H->cap_count;
     CK(cudaStreamEndCapture(s, &g));
     CK(cudaGraphInstantiate(&exec, g, 0));
     cudaGraphDestroy(g);
@@ -750,12 +909,14 @@ void pcg(femh_handle* H, const TB* b, int max_iter, double tol, int iters_out[])
     while (true) {
       if (exec) {
         CK(cudaGraphLaunch(exec, s));
+        H->launches += graph_kernels;
       } else {
         for (int i = 0; i < chunk; ++i) pcg_iteration<TV, TP, TC>(H);
       }
       done += chunk;
       CK(cudaMemcpyAsync(H->state.data(), stt, sizeof(CGState) * H->state.size(), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
+      prof_resolve(H);
       bool any = false;
       for (auto& S : H->state) any |= (S.active != 0);
       if (!any || done > max_iter + chunk) break;
@@ -775,10 +936,16 @@ void true_residual(femh_handle* H, std::vector<double>& rn2) {
   double* r = H->r64 ? H->r64 : (double*)H->cg_r;
   stencil<double, OUT_RESID>(H, L0, false, (const double*)H->x64, r, (const double*)H->b64,
                              (const double*)H->kc64, nullptr, nullptr, 0.0);
-  k_norm2<double><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, r, H->d_part_z, L0.ntot);
-  LAUNCH_CHECK(H);
-  k_sum_slots<<<fin_blocks(H->ncells), 128, 0, s>>>(L0.d_nu_sb, L0.d_nu_se, H->d_part_z, H->d_nrm, H->ncells);
-  LAUNCH_CHECK(H);
+  {
+    Prof prof_(H, "k_norm2", 0.0);
+    k_norm2<double><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, r, H->d_part_z, L0.ntot);
+    LAUNCH_CHECK(H);
+  }
+  {
+    Prof prof_(H, "k_sum_slots", 0.0);
+    k_sum_slots<<<fin_blocks(H->ncells), 128, 0, s>>>(L0.d_nu_sb, L0.d_nu_se, H->d_part_z, H->d_nrm, H->ncells);
+    LAUNCH_CHECK(H);
+  }
   rn2.assign(H->ncells * kNumRhs, 0.0);
   CK(cudaMemcpyAsync(rn2.data(), H->d_nrm, sizeof(double) * rn2.size(), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -787,10 +954,16 @@ void true_residual(femh_handle* H, std::vector<double>& rn2) {
 void norms_of(femh_handle* H, const double* v, std::vector<double>& n2) {
   Level& L0 = H->levels[0];
   cudaStream_t s = H->stream;
-  k_norm2<double><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, v, H->d_part_z, L0.ntot);
-  LAUNCH_CHECK(H);
-  k_sum_slots<<<fin_blocks(H->ncells), 128, 0, s>>>(L0.d_nu_sb, L0.d_nu_se, H->d_part_z, H->d_nrm, H->ncells);
-  LAUNCH_CHECK(H);
+  {
+    Prof prof_(H, "k_norm2", 0.0);
+    k_norm2<double><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, v, H->d_part_z, L0.ntot);
+    LAUNCH_CHECK(H);
+  }
+  {
+    Prof prof_(H, "k_sum_slots", 0.0);
+    k_sum_slots<<<fin_blocks(H->ncells), 128, 0, s>>>(L0.d_nu_sb, L0.d_nu_se, H->d_part_z, H->d_nrm, H->ncells);
+    LAUNCH_CHECK(H);
+  }
   n2.assign(H->ncells * kNumRhs, 0.0);
   CK(cudaMemcpyAsync(n2.data(), H->d_nrm, sizeof(double) * n2.size(), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -847,13 +1020,23 @@ void solve_all(femh_handle* H, std::vector<femh_solve_info>& infos) {
         pcg<float, float, float, double>(H, H->r64, c.max_iter, c.inner_tol, iters.data());
       for (int t = 0; t < nc * kNumRhs; ++t)
         if (H->state[t].status == CG_BREAKDOWN && H->state[t].iters == 0) outer_on[t] = 0;
-      k_dc_accum<float><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->x64, (const float*)H->cg_x,
+      {
+        Prof prof_(H, "k_dc_accum", 0.0);
+        k_dc_accum<float><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->x64, (const float*)H->cg_x,
                                                           H->d_state, L0.ntot);
-      LAUNCH_CHECK(H);
+        LAUNCH_CHECK(H);
+      }
       true_residual(H, rn2);
       for (int t = 0; t < nc * kNumRhs; ++t) {
         const double rel = bn2[t] > 0 ? std::sqrt(rn2[t] / bn2[t]) : 0.0;
         if (rel < c.tol) outer_on[t] = 0;
+      }
+      if (verbose()) {
+        std::fprintf(stderr, "[femh] outer %d:", outer_done);
+        for (int t = 0; t < std::min(nc * kNumRhs, 6); ++t)
+          std::fprintf(stderr, " (%d it, inner %.1e, true %.2e)", H->state[t].iters, H->state[t].rel,
+                       bn2[t] > 0 ? std::sqrt(rn2[t] / bn2[t]) : 0.0);
+        std::fprintf(stderr, "\n");
       }
     }
     for (int t = 0; t < nc * kNumRhs; ++t) {
@@ -894,12 +1077,18 @@ void energy_C(femh_handle* H, std::vector<double>& C, std::vector<double>& dens)
   a.ntot = L0.ntot;
   a.k = H->hk;
   a.law = make_law(H->cfg);
-  k_energy<EN_C><<<(unsigned)L0.all.nu.size(), 128, 0, s>>>(a);
-  LAUNCH_CHECK(H);
+  {
+    Prof prof_(H, "k_energy", 0.0);
+    k_energy<EN_C><<<(unsigned)L0.all.nu.size(), 128, 0, s>>>(a);
+    LAUNCH_CHECK(H);
+  }
   double* d_dens = H->d_nrm;
-  k_energy_fin<<<cdiv((long long)H->ncells * 22, 128), 128, 0, s>>>(L0.d_cells, L0.d_nu_sb, L0.d_nu_se,
+  {
+    Prof prof_(H, "k_energy_fin", 0.0);
+    k_energy_fin<<<cdiv((long long)H->ncells * 22, 128), 128, 0, s>>>(L0.d_cells, L0.d_nu_sb, L0.d_nu_se,
                                                                    H->d_part_e, H->d_C, d_dens, H->ncells);
-  LAUNCH_CHECK(H);
+    LAUNCH_CHECK(H);
+  }
   C.assign(H->ncells * 36, 0.0);
   dens.assign(H->ncells, 0.0);
   CK(cudaMemcpyAsync(C.data(), H->d_C, sizeof(double) * C.size(), cudaMemcpyDeviceToHost, s));
@@ -1105,8 +1294,11 @@ femh_status femh_homogenize_batch(femh_handle* H, int ncell, const femh_cell* ce
       a.ntot = L0.ntot;
       a.k = H->hk;
       a.law = make_law(H->cfg);
-      k_energy<EN_GRAD><<<(unsigned)L0.all.nu.size(), 128, 0, H->stream>>>(a);
-      LAUNCH_CHECK(H);
+      {
+        Prof prof_(H, "k_energy", 0.0);
+        k_energy<EN_GRAD><<<(unsigned)L0.all.nu.size(), 128, 0, H->stream>>>(a);
+        LAUNCH_CHECK(H);
+      }
       to_host_or_dev(H, dLdrho, H->d_out, H->nvox, 0);
     }
   });
@@ -1137,8 +1329,11 @@ femh_status femh_homogenize_grad(femh_handle* H, const double dLdC[36], double* 
     a.ntot = L0.ntot;
     a.k = H->hk;
     a.law = make_law(H->cfg);
-    k_energy<EN_GRAD><<<(unsigned)L0.all.nu.size(), 128, 0, H->stream>>>(a);
-    LAUNCH_CHECK(H);
+    {
+      Prof prof_(H, "k_energy", 0.0);
+      k_energy<EN_GRAD><<<(unsigned)L0.all.nu.size(), 128, 0, H->stream>>>(a);
+      LAUNCH_CHECK(H);
+    }
     to_host_or_dev(H, dLdrho, H->d_out, H->nvox, out_on_device);
   });
 }
@@ -1161,8 +1356,11 @@ femh_status femh_dCdrho(femh_handle* H, double* out, int out_on_device) {
     a.ntot = L0.ntot;
     a.k = H->hk;
     a.law = make_law(H->cfg);
-    k_energy<EN_DCDRHO><<<(unsigned)L0.all.nu.size(), 128, 0, H->stream>>>(a);
-    LAUNCH_CHECK(H);
+    {
+      Prof prof_(H, "k_energy", 0.0);
+      k_energy<EN_DCDRHO><<<(unsigned)L0.all.nu.size(), 128, 0, H->stream>>>(a);
+      LAUNCH_CHECK(H);
+    }
     to_host_or_dev(H, out, H->d_out, 21 * H->nvox, out_on_device);
   });
 }
@@ -1177,9 +1375,12 @@ femh_status femh_full_field(femh_handle* H, int I, double* u_out, int out_on_dev
     const long long n = 3LL * (cd.nx + 1) * (cd.ny + 1) * (cd.nz + 1);
     double* tmp = H->d_out;   // 21*nvox >= 3 (n+1)^3 for n >= 2
     if (n > 21 * H->nvox) throw FemhError{FEMH_E_ARG, "cell too small for the full-field buffer"};
-    k_full_field<<<cdiv(n / 3, 256), 256, 0, H->stream>>>(H->levels[0].d_cells, 0, H->x64, I, tmp,
+    {
+      Prof prof_(H, "k_full_field", 0.0);
+      k_full_field<<<cdiv(n / 3, 256), 256, 0, H->stream>>>(H->levels[0].d_cells, 0, H->x64, I, tmp,
                                                           H->levels[0].ntot);
-    LAUNCH_CHECK(H);
+      LAUNCH_CHECK(H);
+    }
     to_host_or_dev(H, u_out, tmp, n, out_on_device);
   });
 }
@@ -1192,8 +1393,11 @@ femh_status femh_fluctuation(femh_handle* H, double* chi_out, int out_on_device)
     CK(cudaSetDevice(H->device));
     const long long nn = H->nvox;
     double* tmp = H->d_out;
-    k_layout<true><<<cdiv(18 * nn, 256), 256, 0, H->stream>>>(H->x64, tmp, 0, nn, H->levels[0].ntot);
-    LAUNCH_CHECK(H);
+    {
+      Prof prof_(H, "k_layout", 0.0);
+      k_layout<true><<<cdiv(18 * nn, 256), 256, 0, H->stream>>>(H->x64, tmp, 0, nn, H->levels[0].ntot);
+      LAUNCH_CHECK(H);
+    }
     to_host_or_dev(H, chi_out, tmp, 18 * nn, out_on_device);
   });
 }
@@ -1211,17 +1415,26 @@ femh_status femh_apply_operator(femh_handle* H, int nx, int ny, int nz, double h
     CK(cudaMemcpyAsync(H->rho_in, rho, sizeof(double) * nn, k_in, s));
     Level& L0 = H->levels[0];
     const MatLaw law = make_law(H->cfg);
-    k_coef<double><<<(unsigned)L0.all.nu.size(), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->rho_in, law, H->kc64,
+    {
+      Prof prof_(H, "k_coef", 0.0);
+      k_coef<double><<<(unsigned)L0.all.nu.size(), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->rho_in, law, H->kc64,
                                                               (double*)nullptr, H->rho_used);
-    LAUNCH_CHECK(H);
+      LAUNCH_CHECK(H);
+    }
     double* tmp = H->d_out;
     CK(cudaMemcpyAsync(tmp, u, sizeof(double) * 18 * nn, k_in, s));
-    k_layout<false><<<cdiv(18 * nn, 256), 256, 0, s>>>(tmp, H->x64, 0, nn, L0.ntot);
-    LAUNCH_CHECK(H);
+    {
+      Prof prof_(H, "k_layout", 0.0);
+      k_layout<false><<<cdiv(18 * nn, 256), 256, 0, s>>>(tmp, H->x64, 0, nn, L0.ntot);
+      LAUNCH_CHECK(H);
+    }
     stencil<double, OUT_APPLY>(H, L0, false, (const double*)H->x64, H->b64, (const double*)nullptr,
                                (const double*)H->kc64, nullptr, nullptr, 0.0);
-    k_layout<true><<<cdiv(18 * nn, 256), 256, 0, s>>>(H->b64, tmp, 0, nn, L0.ntot);
-    LAUNCH_CHECK(H);
+    {
+      Prof prof_(H, "k_layout", 0.0);
+      k_layout<true><<<cdiv(18 * nn, 256), 256, 0, s>>>(H->b64, tmp, 0, nn, L0.ntot);
+      LAUNCH_CHECK(H);
+    }
     to_host_or_dev(H, y, tmp, 18 * nn, on_device);
     H->solved = false;
   });
@@ -1240,5 +1453,33 @@ femh_status femh_set_stream(femh_handle* H, void* stream) {
 }
 
 long long femh_kernel_launches(const femh_handle* H) { return H ? H->launches : -1; }
+
+femh_status femh_profile(femh_handle* H, int enable) {
+  if (!H) return FEMH_E_ARG;
+  return guard(H, [&] {
+    prof_resolve(H);
+    H->prof = enable != 0;
+    H->kstats.clear();
+  });
+}
+
+femh_status femh_profile_read(femh_handle* H, femh_kernel_stat* out, int max, int* n) {
+  if (!H || !n || (max > 0 && !out)) return FEMH_E_ARG;
+  return guard(H, [&] {
+    prof_resolve(H);
+    int i = 0;
+    for (auto& kv : H->kstats) {
+      if (kv.second.launches == 0) continue;
+      if (i < max) {
+        std::snprintf(out[i].name, sizeof out[i].name, "%s", kv.first.c_str());
+        out[i].launches = kv.second.launches;
+        out[i].total_ms = kv.second.ms;
+        out[i].bytes = kv.second.bytes;
+      }
+      ++i;
+    }
+    *n = i;
+  });
+}
 
 }  // extern "C"

@@ -63,11 +63,15 @@ __global__ void k_coef(const CellDesc* cells, const NodeUnit* units, const doubl
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
     double r = rho[cd.off + n];
     r = fmin(fmax(r, law.rho_min), law.rho_max);
-    if (law.rho_bf16) r = (double)__bfloat162float(__float2bfloat16_rn((float)r));
     const double kc = law_coef(law, r) * cd.h;
     if (rho_used) rho_used[cd.off + n] = r;
     if (kc64) kc64[cd.off + n] = kc;
-    if (kc2) kc2[cd.off + n] = (TC2)kc;
+    if (kc2) {
+      // the inner (FP32) operator may see rho rounded to bf16; the FP64
+      // operator that defines the solution always uses rho as given
+      const double rb = law.rho_bf16 ? (double)__bfloat162float(__float2bfloat16_rn((float)r)) : r;
+      kc2[cd.off + n] = (TC2)(law.rho_bf16 ? law_coef(law, rb) * cd.h : kc);
+    }
   }
 }
 
@@ -235,21 +239,32 @@ __global__ void k_cg_dir(const CellDesc* cells, const NodeUnit* units, TP* p, co
   }
 }
 
-// Sum of the partials of one (cell, rhs) over the cell's slot range, fixed order.
+// Sum of the partials of one (cell, rhs) over the cell's slot range: one warp,
+// lane-strided then a shuffle tree (fixed order: deterministic).  Valid in all lanes.
 __device__ __forceinline__ double sum_slots(const double* part, int b, int e, int rhs, int stride,
                                             int comp) {
+  const int lane = threadIdx.x & 31;
   double s = 0.0;
-  for (int t = b; t < e; ++t) s += part[((long long)t * kNumRhs + rhs) * stride + comp];
+  for (int t = b + lane; t < e; t += 32) s += part[((long long)t * kNumRhs + rhs) * stride + comp];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   return s;
 }
+
+// One warp per (cell, rhs) in the finalisation kernels.
+#define FIN_PROLOGUE                                                         \
+  const int t = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5); \
+  const bool lead = (threadIdx.x & 31) == 0;                                 \
+  if (t >= ncells * kNumRhs) return;                                         \
+  const int cell = t / kNumRhs, rhs = t % kNumRhs;                           \
+  (void)cell;                                                                \
+  (void)rhs;
 
 // After k_cg_init: bnorm2, rz (Jacobi) / rr; decide which (cell, rhs) run.
 // One thread per (cell, rhs).
 __global__ void k_fin_init(CGState* stt, const int* slot_begin, const int* slot_end,
                            const double* part, int ncells, int jacobi) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ncells * kNumRhs) return;
-  const int cell = t / kNumRhs, rhs = t % kNumRhs;
+  FIN_PROLOGUE
   CGState S = stt[t];
   if (!S.active) return;
   const double rr = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 2, 0);
@@ -259,27 +274,23 @@ __global__ void k_fin_init(CGState* stt, const int* slot_begin, const int* slot_
   S.iters = 0;
   S.rel = (rr > 0.0) ? 1.0 : 0.0;
   if (!(rr > 0.0)) { S.active = 0; S.status = CG_CONVERGED; }
-  stt[t] = S;
+  if (lead) stt[t] = S;
 }
 
 // rz for the multigrid preconditioner at start (z0 . r from the V-cycle's last sweep).
 __global__ void k_fin_rz(CGState* stt, const int* slot_begin, const int* slot_end,
                          const double* part, int ncells) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ncells * kNumRhs) return;
-  const int cell = t / kNumRhs, rhs = t % kNumRhs;
+  FIN_PROLOGUE
   CGState S = stt[t];
   if (!S.active) return;
   S.rz = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 1, 0);
-  stt[t] = S;
+  if (lead) stt[t] = S;
 }
 
 // alpha = rz / (p . K p); breakdown if p.Kp <= 0 or not finite.
 __global__ void k_fin_alpha(CGState* stt, const int* slot_begin, const int* slot_end,
                             const double* part, int ncells) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ncells * kNumRhs) return;
-  const int cell = t / kNumRhs, rhs = t % kNumRhs;
+  FIN_PROLOGUE
   CGState S = stt[t];
   if (!S.active) return;
   const double pq = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 1, 0);
@@ -291,16 +302,14 @@ __global__ void k_fin_alpha(CGState* stt, const int* slot_begin, const int* slot
   } else {
     S.alpha = S.rz / pq;
   }
-  stt[t] = S;
+  if (lead) stt[t] = S;
 }
 
 // After the update (+ preconditioner): convergence test and beta.
 // jacobi: rz_new from the update partials; else from the V-cycle partials.
 __global__ void k_fin_beta(CGState* stt, const int* slot_begin, const int* slot_end,
                            const double* part_upd, const double* part_rz, int ncells, int jacobi) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ncells * kNumRhs) return;
-  const int cell = t / kNumRhs, rhs = t % kNumRhs;
+  FIN_PROLOGUE
   CGState S = stt[t];
   if (!S.active) return;
   const int b = slot_begin[cell], e = slot_end[cell];
@@ -322,7 +331,7 @@ __global__ void k_fin_beta(CGState* stt, const int* slot_begin, const int* slot_
     S.beta = rzn / S.rz;
     S.rz = rzn;
   }
-  stt[t] = S;
+  if (lead) stt[t] = S;
 }
 
 // ---------------------------------------------------------- multigrid ---
@@ -713,10 +722,9 @@ __global__ void k_norm2(const CellDesc* cells, const NodeUnit* units, const TV* 
 
 __global__ void k_sum_slots(const int* slot_begin, const int* slot_end, const double* part, double* out,
                             int ncells) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ncells * kNumRhs) return;
-  const int cell = t / kNumRhs, rhs = t % kNumRhs;
-  out[t] = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 1, 0);
+  FIN_PROLOGUE
+  const double v = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 1, 0);
+  if (lead) out[t] = v;
 }
 
 // Full-cell displacement on (nx+1)(ny+1)(nz+1) nodes for load case I: periodic

@@ -31,7 +31,7 @@ JACOBI_PCG, GMG_PCG = 0, 1
 EXPORTS = (
     "femh_config_default", "femh_create", "femh_destroy", "femh_homogenize", "femh_homogenize_grad",
     "femh_dCdrho", "femh_full_field", "femh_fluctuation", "femh_apply_operator", "femh_homogenize_batch",
-    "femh_last_error", "femh_set_stream", "femh_kernel_launches",
+    "femh_last_error", "femh_set_stream", "femh_kernel_launches", "femh_profile", "femh_profile_read",
 )
 
 
@@ -68,6 +68,11 @@ class _Cell(ctypes.Structure):
                 ("rho", ctypes.POINTER(ctypes.c_double))]
 
 
+class _KStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 64), ("launches", ctypes.c_longlong), ("total_ms", ctypes.c_double),
+                ("bytes", ctypes.c_double)]
+
+
 _lib = None
 
 
@@ -94,6 +99,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.femh_set_stream.argtypes = [vp, vp]
     L.femh_kernel_launches.argtypes = [vp]
     L.femh_kernel_launches.restype = ctypes.c_longlong
+    L.femh_profile.argtypes = [vp, ip]
+    L.femh_profile_read.argtypes = [vp, ctypes.POINTER(_KStat), ip, ctypes.POINTER(ctypes.c_int)]
     _lib = L
     return L
 
@@ -184,6 +191,18 @@ class Engine:
     @property
     def kernel_launches(self) -> int:
         return int(self.lib.femh_kernel_launches(self.h))
+
+    def profile(self, enable: bool = True):
+        """Per-kernel CUDA-event timing (graphs off while enabled); clears stats."""
+        self._check(self.lib.femh_profile(self.h, int(enable)))
+
+    def profile_read(self) -> list[dict]:
+        n = ctypes.c_int()
+        self._check(self.lib.femh_profile_read(self.h, None, 0, ctypes.byref(n)))
+        arr = (_KStat * max(n.value, 1))()
+        self._check(self.lib.femh_profile_read(self.h, arr, n.value, ctypes.byref(n)))
+        return [{"name": a.name.decode(), "launches": a.launches, "total_ms": a.total_ms, "bytes": a.bytes}
+                for a in arr[:n.value]]
 
     def set_stream(self, stream_ptr: int | None):
         self._check(self.lib.femh_set_stream(self.h, ctypes.c_void_p(stream_ptr or 0)))

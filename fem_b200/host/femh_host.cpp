@@ -1,0 +1,293 @@
+// femh_host.cpp -- the reference-facing C++ layer over the C ABI (see
+// femh_host.hpp for the interfaces it mirrors).
+#include "femh_host.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <fstream>
+
+namespace femh_host {
+
+namespace {
+void check(femh_handle* h, int st, bool allow_unconverged = false) {
+  if (st == FEMH_OK || (allow_unconverged && st == FEMH_E_NOT_CONVERGED)) return;
+  char buf[512] = {0};
+  if (h) femh_last_error(h, buf, sizeof buf);
+  else std::snprintf(buf, sizeof buf, "engine creation failed (no CUDA device or bad config)");
+  throw Error(st, "femh error " + std::to_string(st) + ": " + buf);
+}
+}  // namespace
+
+// ---------------------------------------------------------- PiecewiseConstant3D
+void PiecewiseConstant3D::allocate(int nx, int ny, int nz) {
+  gridSize[0] = nx;
+  gridSize[1] = ny;
+  gridSize[2] = nz;
+  param.assign((size_t)nx * ny * nz, 1.0);
+}
+
+int PiecewiseConstant3D::index(const std::array<double, 3>& x) const {
+  int idx[3];
+  for (int d = 0; d < 3; ++d) idx[d] = std::min(std::max((int)(x[d] * gridSize[d]), 0), gridSize[d] - 1);
+  return (idx[0] * gridSize[1] + idx[1]) * gridSize[2] + idx[2];
+}
+
+double PiecewiseConstant3D::f(const std::array<double, 3>& x) { return param[index(x)]; }
+
+std::vector<SparseEntry> PiecewiseConstant3D::df(const std::array<double, 3>& x) { return {{index(x), 1.0}}; }
+
+// -------------------------------------------------------------------- FEM3DFun
+FEM3DFun::FEM3DFun() {}
+
+FEM3DFun::~FEM3DFun() {
+  if (h_) femh_destroy(h_);
+}
+
+void FEM3DFun::ensure_handle() {
+  if (h_) return;
+  femh_config c;
+  femh_config_default(&c);
+  c.interp = FEMH_INTERP_RAMP3;   // coef x/(3-2x) of fast_fem/FEM3DFun.cpp:20-27
+  c.E_s = E;
+  c.nu = nu;
+  c.rho_min = 1e-3;               // Clamp(field->f, 1e-3, 1), FEM3DFun.cpp:147
+  c.rho_max = 1.0;
+  c.precision = precision;
+  c.solver = solver;
+  check(nullptr, femh_create(&h_, &c));
+}
+
+void FEM3DFun::init(const std::vector<double>& x0) {
+  param = x0;
+  ensure_handle();
+}
+
+void FEM3DFun::setParam(const std::vector<double>& x0) {
+  if (!field) throw Error(FEMH_E_STATE, "FEM3DFun::setParam needs a field");
+  ensure_handle();
+  param = x0;
+  for (size_t i = 0; i < field->param.size() && i < x0.size(); ++i) field->setParam((int)i, x0[i]);
+  const int nx = gridSize[0], ny = gridSize[1], nz = gridSize[2];
+  distribution.assign((size_t)nx * ny * nz, 0.0);
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        const std::array<double, 3> x = {(i + 0.5) / nx, (j + 0.5) / ny, (k + 0.5) / nz};
+        distribution[((size_t)i * ny + j) * nz + k] = std::min(std::max(field->f(x), 1e-3), 1.0);
+      }
+  check(h_, femh_homogenize(h_, nx, ny, nz, 1.0 / nx, distribution.data(), 0, G.data(), &lastInfo), true);
+  density = 0.0;
+  for (double d : distribution) density += d;
+  density /= (double)distribution.size();
+}
+
+double FEM3DFun::f() {
+  double sum = 0.0;
+  for (int t = 0; t < 36; ++t) sum += wG[t] * (G[t] - G0[t]) * (G[t] - G0[t]);
+  return 0.5 * sum + 0.5 * mw * (density - m0) * (density - m0);
+}
+
+std::vector<double> FEM3DFun::df() {
+  const int nx = gridSize[0], ny = gridSize[1], nz = gridSize[2];
+  const size_t nv = (size_t)nx * ny * nz;
+  std::vector<double> dfddist(nv, 0.0);
+  double dLdC[36];
+  for (int t = 0; t < 36; ++t) dLdC[t] = wG[t] * (G[t] - G0[t]);
+  check(h_, femh_homogenize_grad(h_, dLdC, dfddist.data(), 0));
+  const double dm = (mw / (double)nv) * (density - m0);
+  for (auto& v : dfddist) v += dm;
+  std::vector<double> grad(param.size(), 0.0);
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        const std::array<double, 3> x = {(i + 0.5) / nx, (j + 0.5) / ny, (k + 0.5) / nz};
+        const double g = dfddist[((size_t)i * ny + j) * nz + k];
+        for (const auto& e : field->df(x))
+          if (e.first >= 0 && (size_t)e.first < grad.size()) grad[e.first] += g * e.second;
+      }
+  return grad;
+}
+
+// ----------------------------------------------- NumericalCoarseningUsingMultigrid
+void fromLamesParametersToYoungModulusPoissonRatio(double lambda, double mu, double& E, double& nu) {
+  E = mu * (3 * lambda + 2 * mu) / (lambda + mu);
+  nu = lambda / (2 * (lambda + mu));
+}
+
+void repMaterialAssignment(int nx, int ny, int nz, const std::vector<int>& in, int repX, int repY, int repZ,
+                           int sub, std::vector<int>& out) {
+  const int NX = repX * nx * sub, NY = repY * ny * sub, NZ = repZ * nz * sub;
+  out.assign((size_t)NX * NY * NZ, -1);
+  for (int m = 0; m < nx; ++m)
+    for (int n = 0; n < ny; ++n)
+      for (int p = 0; p < nz; ++p) {
+        const int v = in[((size_t)m * ny + n) * nz + p];
+        for (int i = 0; i < repX; ++i)
+          for (int j = 0; j < repY; ++j)
+            for (int k = 0; k < repZ; ++k)
+              for (int a = 0; a < sub; ++a)
+                for (int b = 0; b < sub; ++b)
+                  for (int c = 0; c < sub; ++c) {
+                    const int X = i * sub * nx + m * sub + a;
+                    const int Y = j * sub * ny + n * sub + b;
+                    const int Z = k * sub * nz + p * sub + c;
+                    out[((size_t)X * NY + Y) * NZ + Z] = v;
+                  }
+      }
+}
+
+NumericalCoarseningUsingMultigrid::NumericalCoarseningUsingMultigrid() {}
+
+NumericalCoarseningUsingMultigrid::~NumericalCoarseningUsingMultigrid() {
+  if (h_) femh_destroy(h_);
+}
+
+void NumericalCoarseningUsingMultigrid::init(int N[3], int iNbBlockRep, int iNbSubdiv,
+                                             const std::vector<BaseMaterial>& mats, StructureType) {
+  if (mats.size() < 2) throw Error(FEMH_E_ARG, "two base materials are required");
+  m_nbBlockRep = iNbBlockRep;
+  m_nbSubdiv = iNbSubdiv;
+  // The reference swaps materials 0 and 1 and assigns material id 0 to every
+  // cell, so K0 is the stiffness of base material 1; the per-cell coefficient
+  // is 1 for material 1 and m_densityMin otherwise
+  // (NumericalCoarseningUsingMultiGrid.cpp:170-193, 229-241).
+  fromLamesParametersToYoungModulusPoissonRatio(mats[1].lambda, mats[1].mu, m_E, m_nu);
+  if (h_) femh_destroy(h_);
+  h_ = nullptr;
+  femh_config c;
+  femh_config_default(&c);
+  c.interp = FEMH_INTERP_BINARY;
+  c.bin_hi = m_E;
+  c.bin_lo = m_E * (m_useVariableDensity ? m_densityMin : 1.0);
+  c.nu = m_nu;
+  check(nullptr, femh_create(&h_, &c));
+  (void)N;
+}
+
+void NumericalCoarseningUsingMultigrid::append(const double C[36], const std::vector<int>& mats,
+                                               const std::vector<double>& dens, StructureType t,
+                                               std::vector<double>& tv, std::vector<double>& pv) {
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j <= i; ++j) tv.push_back(C[i * 6 + j]);
+  if (t != Cubic) throw Error(FEMH_E_ARG, "only Cubic structures derive (rho, E, nu, G), as in the reference");
+  double r = 0.0;
+  for (int m : mats) r += dens.at(m);
+  r /= (double)mats.size();
+  const double Gs = C[3 * 6 + 3];
+  const double a = C[0 * 6 + 1] / C[0];
+  const double nuxy = a / (1 + a);
+  const double Ey = C[0 * 6 + 1] * (1 + nuxy) * (1 - 2 * nuxy) / nuxy;
+  pv.push_back(r);
+  pv.push_back(Ey);
+  pv.push_back(nuxy);
+  pv.push_back(Gs);
+}
+
+void NumericalCoarseningUsingMultigrid::computeCoarsenedElasticityTensorAndParameters3D(
+    const std::vector<int>& iMaterials, int N[3], const std::vector<double>& iDens, StructureType t,
+    std::vector<double>& tv, std::vector<double>& pv) {
+  if (!h_) throw Error(FEMH_E_STATE, "init() first");
+  std::vector<int> cells;
+  repMaterialAssignment(N[0], N[1], N[2], iMaterials, m_nbBlockRep, m_nbBlockRep, m_nbBlockRep, m_nbSubdiv, cells);
+  const int n[3] = {N[0] * m_nbBlockRep * m_nbSubdiv, N[1] * m_nbBlockRep * m_nbSubdiv,
+                    N[2] * m_nbBlockRep * m_nbSubdiv};
+  std::vector<double> rho(cells.size());
+  for (size_t i = 0; i < cells.size(); ++i) rho[i] = cells[i] == 1 ? 1.0 : 0.0;
+  double C[36];
+  check(h_, femh_homogenize(h_, n[0], n[1], n[2], 1.0 / n[0], rho.data(), 0, C, &lastInfo), true);
+  append(C, iMaterials, iDens, t, tv, pv);
+}
+
+void NumericalCoarseningUsingMultigrid::computeBatch(const std::vector<std::vector<int>>& iMaterials, int N[3],
+                                                     const std::vector<double>& iDens, StructureType t,
+                                                     std::vector<double>& tv, std::vector<double>& pv) {
+  if (!h_) throw Error(FEMH_E_STATE, "init() first");
+  const size_t nc = iMaterials.size();
+  if (nc == 0) return;
+  const int n[3] = {N[0] * m_nbBlockRep * m_nbSubdiv, N[1] * m_nbBlockRep * m_nbSubdiv,
+                    N[2] * m_nbBlockRep * m_nbSubdiv};
+  std::vector<std::vector<double>> rho(nc);
+  std::vector<femh_cell> cells(nc);
+  for (size_t c = 0; c < nc; ++c) {
+    std::vector<int> m;
+    repMaterialAssignment(N[0], N[1], N[2], iMaterials[c], m_nbBlockRep, m_nbBlockRep, m_nbBlockRep, m_nbSubdiv, m);
+    rho[c].resize(m.size());
+    for (size_t i = 0; i < m.size(); ++i) rho[c][i] = m[i] == 1 ? 1.0 : 0.0;
+    cells[c] = femh_cell{n[0], n[1], n[2], 1.0 / n[0], rho[c].data()};
+  }
+  std::vector<double> C(36 * nc);
+  std::vector<femh_solve_info> infos(nc);
+  check(h_, femh_homogenize_batch(h_, (int)nc, cells.data(), C.data(), nullptr, nullptr, infos.data()), true);
+  for (size_t c = 0; c < nc; ++c) append(&C[36 * c], iMaterials[c], iDens, t, tv, pv);
+  if (nc) lastInfo = infos.back();
+}
+
+// ------------------------------------------------------------ binary files
+template <class T>
+bool writeBinary(const std::string& file, const std::vector<T>& v) {
+  std::ofstream f(file, std::ios::binary);
+  if (!f) return false;
+  const int32_t n = (int32_t)v.size();
+  f.write((const char*)&n, sizeof n);
+  if (n > 0) f.write((const char*)v.data(), sizeof(T) * n);
+  return (bool)f;
+}
+
+template <class T>
+bool readBinary(const std::string& file, std::vector<T>& v) {
+  std::ifstream f(file, std::ios::binary);
+  if (!f) return false;
+  int32_t n = 0;
+  f.read((char*)&n, sizeof n);
+  if (!f || n < 0) return false;
+  v.resize(n);
+  if (n > 0) f.read((char*)v.data(), sizeof(T) * n);
+  return (bool)f;
+}
+
+template <class T>
+bool writeBinary(const std::string& file, const std::vector<std::vector<T>>& v) {
+  std::ofstream f(file, std::ios::binary);
+  if (!f) return false;
+  const int32_t n = (int32_t)v.size();
+  f.write((const char*)&n, sizeof n);
+  for (const auto& row : v) {
+    const int32_t m = (int32_t)row.size();
+    f.write((const char*)&m, sizeof m);
+    if (m > 0) f.write((const char*)row.data(), sizeof(T) * m);
+  }
+  return (bool)f;
+}
+
+template <class T>
+bool readBinary(const std::string& file, std::vector<std::vector<T>>& v) {
+  std::ifstream f(file, std::ios::binary);
+  if (!f) return false;
+  int32_t n = 0;
+  f.read((char*)&n, sizeof n);
+  if (!f || n < 0) return false;
+  v.assign(n, {});
+  for (auto& row : v) {
+    int32_t m = 0;
+    f.read((char*)&m, sizeof m);
+    if (!f || m < 0) return false;
+    row.resize(m);
+    if (m > 0) f.read((char*)row.data(), sizeof(T) * m);
+  }
+  return (bool)f;
+}
+
+template bool writeBinary<float>(const std::string&, const std::vector<float>&);
+template bool writeBinary<int>(const std::string&, const std::vector<int>&);
+template bool writeBinary<double>(const std::string&, const std::vector<double>&);
+template bool readBinary<float>(const std::string&, std::vector<float>&);
+template bool readBinary<int>(const std::string&, std::vector<int>&);
+template bool readBinary<double>(const std::string&, std::vector<double>&);
+template bool writeBinary<float>(const std::string&, const std::vector<std::vector<float>>&);
+template bool writeBinary<int>(const std::string&, const std::vector<std::vector<int>>&);
+template bool readBinary<float>(const std::string&, std::vector<std::vector<float>>&);
+template bool readBinary<int>(const std::string&, std::vector<std::vector<int>>&);
+
+}  // namespace femh_host

@@ -1,0 +1,150 @@
+// femh_host.hpp -- C++ host layer over the C ABI (include/femh.h) that mirrors
+// the reference's homogenization interfaces, so reference callers switch by
+// relinking:
+//   - RealFun / RealField / PiecewiseConstant3D / FEM3DFun
+//       (fast_fem/RealFun.hpp:13-50, fast_fem/RealField.hpp, fast_fem/PiecewiseConstant3D.cpp,
+//        fast_fem/FEM3DFun.hpp:13-92 / FEM3DFun.cpp:128-268)
+//   - NumericalCoarseningUsingMultigrid
+//       (SamplesGenerator/NumericalCoarseningUsingMultigrid.h:11-48,
+//        NumericalCoarseningUsingMultiGrid.cpp:134-345)
+//   - computeParametersAndTensorValues (the sample generator's batch call,
+//       SamplesGenerator/SamplesGeneratorImpl.cpp:3683-3752) and the level*.bin
+//       file format (Utilities/include/cfgUtilities.h:780-870).
+// Eigen types of the reference become std::vector<double>; names, argument
+// meaning and outputs are kept.  Every numeric step runs in libfemh.
+#pragma once
+#include <array>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/femh.h"
+
+namespace femh_host {
+
+// Error thrown when the engine reports a failure (the reference asserts or prints).
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// ------------------------------------------------------------- fast_fem ---
+class RealFun {
+ public:
+  std::vector<double> param;
+  std::vector<double> lowerBounds, upperBounds;
+  virtual void init(const std::vector<double>& x0) { param = x0; }
+  virtual void setParam(const std::vector<double>& x0) { param = x0; }
+  virtual double f() = 0;
+  virtual std::vector<double> df() { return {}; }
+  virtual ~RealFun() {}
+};
+
+// Sparse derivative entry (index, value) of a field value w.r.t. its parameters.
+using SparseEntry = std::pair<int, double>;
+
+class RealField {
+ public:
+  std::vector<double> param;
+  virtual double f(const std::array<double, 3>& x) = 0;
+  virtual std::vector<SparseEntry> df(const std::array<double, 3>& x) = 0;
+  virtual void setParam(int i, double v) { param.at(i) = v; }
+  virtual ~RealField() {}
+};
+
+// One parameter per grid cell (fast_fem/PiecewiseConstant3D.cpp).
+class PiecewiseConstant3D : public RealField {
+ public:
+  int gridSize[3] = {0, 0, 0};
+  void allocate(int nx, int ny, int nz);
+  double f(const std::array<double, 3>& x) override;
+  std::vector<SparseEntry> df(const std::array<double, 3>& x) override;
+
+ private:
+  int index(const std::array<double, 3>& x) const;
+};
+
+// Homogenized-stiffness objective on a periodic voxel cell.  G is C^H (both
+// triangles); f = 0.5 sum wG (G-G0)^2 + 0.5 mw (density-m0)^2; df is the
+// adjoint gradient w.r.t. the field parameters.
+class FEM3DFun : public RealFun {
+ public:
+  FEM3DFun();
+  ~FEM3DFun() override;
+  FEM3DFun(const FEM3DFun&) = delete;
+  FEM3DFun& operator=(const FEM3DFun&) = delete;
+
+  // material of the solid (fast_fem: ElasticMaterial(E, nu)), precision/solver
+  double E = 1.0, nu = 0.3;
+  int precision = FEMH_FP64, solver = FEMH_GMG_PCG;
+
+  std::array<double, 36> G{}, G0{}, wG{};
+  double density = 0, m0 = 0, mw = 0;
+  std::vector<int> gridSize{0, 0, 0};
+  RealField* field = nullptr;          // not owned (as in the reference)
+  std::vector<double> distribution;    // per voxel, clamped to [1e-3, 1]
+  femh_solve_info lastInfo{};
+
+  void init(const std::vector<double>& x0) override;
+  void setParam(const std::vector<double>& x0) override;
+  double f() override;
+  std::vector<double> df() override;
+
+ private:
+  femh_handle* h_ = nullptr;
+  void ensure_handle();
+};
+
+// --------------------------------------------------------- SamplesGenerator ---
+struct BaseMaterial {   // StrainLin parameters: param[0] = mu, param[1] = lambda
+  double mu, lambda;
+};
+
+class NumericalCoarseningUsingMultigrid {
+ public:
+  enum StructureType { General, Cubic, Orthotropic };
+
+  NumericalCoarseningUsingMultigrid();
+  ~NumericalCoarseningUsingMultigrid();
+  NumericalCoarseningUsingMultigrid(const NumericalCoarseningUsingMultigrid&) = delete;
+  NumericalCoarseningUsingMultigrid& operator=(const NumericalCoarseningUsingMultigrid&) = delete;
+
+  void setUseVariableDensity(bool v) { m_useVariableDensity = v; }
+  void init(int N[3], int iNbBlockRep, int iNbSubdiv, const std::vector<BaseMaterial>& iBaseMaterials,
+            StructureType iType);
+  // Appends the 21 lower-triangle entries of C^H and, for Cubic, (rho, E, nu_xy, G).
+  void computeCoarsenedElasticityTensorAndParameters3D(const std::vector<int>& iMaterials, int N[3],
+                                                       const std::vector<double>& iBaseMaterialDensities,
+                                                       StructureType iType, std::vector<double>& ioTensorValues,
+                                                       std::vector<double>& ioParameters);
+  // Many structures in one engine call (the sample generator's batch).
+  void computeBatch(const std::vector<std::vector<int>>& iMaterials, int N[3],
+                    const std::vector<double>& iBaseMaterialDensities, StructureType iType,
+                    std::vector<double>& ioTensorValues, std::vector<double>& ioParameters);
+
+  femh_solve_info lastInfo{};
+
+ private:
+  femh_handle* h_ = nullptr;
+  int m_nbBlockRep = 1, m_nbSubdiv = 1;
+  bool m_useVariableDensity = true;
+  double m_densityMin = 1e-4;
+  double m_E = 1.0, m_nu = 0.3;
+  void append(const double C[36], const std::vector<int>& mats, const std::vector<double>& dens,
+              StructureType t, std::vector<double>& tv, std::vector<double>& pv);
+};
+
+// cfgMaterialUtilities::repMaterialAssignment (Utilities/src/cfgMaterialUtilities.cpp:914-956)
+void repMaterialAssignment(int nx, int ny, int nz, const std::vector<int>& iMaterialCombIndices, int repX,
+                           int repY, int repZ, int iNbSubdivisions, std::vector<int>& oMaterials);
+// Lame -> (E, nu)  (Utilities/src/cfgMaterialUtilities.cpp:2945-2949)
+void fromLamesParametersToYoungModulusPoissonRatio(double lambda, double mu, double& E, double& nu);
+
+// level*.bin files: int32 count + raw values; nested vectors count-prefixed.
+template <class T> bool writeBinary(const std::string& file, const std::vector<T>& v);
+template <class T> bool readBinary(const std::string& file, std::vector<T>& v);
+template <class T> bool writeBinary(const std::string& file, const std::vector<std::vector<T>>& v);
+template <class T> bool readBinary(const std::string& file, std::vector<std::vector<T>>& v);
+
+}  // namespace femh_host

@@ -148,9 +148,23 @@ femh_status femh_last_error(const femh_handle* h, char* buf, size_t n);
 /* Stream used by the handle (cudaStream_t as void*); NULL restores its own. */
 femh_status femh_set_stream(femh_handle* h, void* stream);
 
-/* Kernel launches issued by the handle since creation (all are this library's
- * own kernels). */
+/* Kernel executions issued by the handle since creation (all are this
+ * library's own kernels; CUDA-graph replays count every kernel they run). */
 long long femh_kernel_launches(const femh_handle* h);
+
+/* Measurement hooks (no counterpart in the reference, whose only timing is an
+ * ad-hoc wall clock, femlib/src/Timer.cpp).  With profiling on, CUDA graphs are
+ * not captured and every launch is bracketed by CUDA events on the handle's
+ * stream; stats accumulate per kernel class with the algorithmic bytes each
+ * launch must move (inputs read once + outputs written once). */
+typedef struct {
+  char name[64];
+  long long launches;
+  double total_ms;
+  double bytes;
+} femh_kernel_stat;
+femh_status femh_profile(femh_handle* h, int enable);   /* also clears the stats */
+femh_status femh_profile_read(femh_handle* h, femh_kernel_stat* out, int max, int* n);
 
 #ifdef __cplusplus
 }

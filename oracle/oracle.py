@@ -66,6 +66,8 @@ def lib():
             dp, dp, ctypes.POINTER(ctypes.c_int), dp]
         L.fo_homogenize.restype = ctypes.c_int
         L.fo_num_threads.restype = ctypes.c_int
+        L.fo_pcg1.argtypes = [ctypes.c_int] * 3 + [dp, dp, dp, dp, dp, ctypes.c_double, ctypes.c_int, dp]
+        L.fo_pcg1.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -155,6 +157,28 @@ def grad(rho, chi, dLdC, h=None, mat=None) -> np.ndarray:
     lib().fo_grad(nx, ny, nz, h, _p(K0), ctypes.byref(mat), _p(rho), _p(np.ascontiguousarray(chi)),
                   _p(np.ascontiguousarray(dLdC, dtype=np.float64)), _p(out))
     return out
+
+
+def time_pcg(rho, iters: int, mat: Material | None = None, h: float | None = None) -> float:
+    """Seconds per Jacobi-PCG iteration of all six load cases (FP64, OpenMP),
+    measured over `iters` iterations of each load case at the full size."""
+    import time
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    nx, ny, nz = rho.shape
+    h = 1.0 / nx if h is None else h
+    mat = material() if mat is None else mat
+    K0 = k0(1.0, mat.nu, h)
+    c = np.ascontiguousarray(coef(mat, rho))
+    b = rhs(rho.shape, h, K0, c)
+    dinv = np.zeros(rho.shape + (3,))
+    L = lib()
+    L.fo_inv_diag(nx, ny, nz, _p(K0), _p(c), _p(dinv))
+    x = np.zeros(rho.shape + (3,))
+    rel = np.zeros(1)
+    t0 = time.perf_counter()
+    for I in range(6):
+        L.fo_pcg1(nx, ny, nz, _p(K0), _p(c), _p(dinv), _p(np.ascontiguousarray(b[I])), _p(x), 0.0, iters, _p(rel))
+    return (time.perf_counter() - t0) / iters
 
 
 def num_threads() -> int:

@@ -1,0 +1,114 @@
+// test_host.cpp -- exercises the reference-facing C++ layer (femh_host) the way
+// the reference exercises FEM3DFun / NumericalCoarseningUsingMultigrid:
+//   1. FEM3DFun::setParam / f / df with a PiecewiseConstant3D field and the
+//      central-difference check of df (fast_fem/run3d.cpp:291-323 check_df);
+//   2. NumericalCoarseningUsingMultigrid init + computeCoarsened... on a
+//      replicated/subdivided structure (21 tensor values + 4 parameters), and
+//      the batched call against the one-at-a-time call;
+//   3. level*.bin round trip (cfgUtil::writeBinary / readBinary format).
+// Prints one JSON object; tests/test_gpu_host.py checks it (also against the
+// oracle).  Exit code != 0 on a failed in-program check.
+#include <cmath>
+#include <cstdio>
+#include <random>
+#include <vector>
+
+#include "../../fem_b200/host/femh_host.hpp"
+
+using namespace femh_host;
+
+static void print_vec(const char* key, const std::vector<double>& v, bool last = false) {
+  std::printf("\"%s\": [", key);
+  for (size_t i = 0; i < v.size(); ++i) std::printf("%s%.17g", i ? ", " : "", v[i]);
+  std::printf("]%s\n", last ? "" : ",");
+}
+
+int main() {
+  int fails = 0;
+  std::printf("{\n");
+  // ---------------------------------------------------------------- 1
+  const int n = 8;
+  PiecewiseConstant3D field;
+  field.allocate(n, n, n);
+  std::mt19937 rng(7);
+  std::uniform_real_distribution<double> U(0.2, 0.95);
+  std::vector<double> x0(n * n * n);
+  for (auto& v : x0) v = U(rng);
+  FEM3DFun fun;
+  fun.gridSize = {n, n, n};
+  fun.field = &field;
+  fun.E = 1.0;
+  fun.nu = 0.3;
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) {
+      fun.wG[i * 6 + j] = (i <= 2 && j <= 2) ? 1.0 : 0.5;
+      fun.G0[i * 6 + j] = (i == j) ? 0.05 : 0.0;
+    }
+  fun.m0 = 0.4;
+  fun.mw = 0.1;
+  fun.init(x0);
+  fun.setParam(x0);
+  const double f0 = fun.f();
+  std::vector<double> G(fun.G.begin(), fun.G.end());
+  std::vector<double> g = fun.df();
+  const double hstep = 1e-6;
+  std::vector<double> fd, an;
+  for (int t = 0; t < 4; ++t) {
+    const int k = (int)(rng() % x0.size());
+    std::vector<double> xp = x0, xm = x0;
+    xp[k] += hstep;
+    xm[k] -= hstep;
+    fun.setParam(xp);
+    const double fp = fun.f();
+    fun.setParam(xm);
+    const double fm = fun.f();
+    fd.push_back((fp - fm) / (2 * hstep));
+    an.push_back(g[k]);
+  }
+  fun.setParam(x0);
+  std::printf("\"f\": %.17g,\n", f0);
+  std::printf("\"density\": %.17g,\n", fun.density);
+  print_vec("G", G);
+  print_vec("x0", x0);
+  print_vec("df_fd", fd);
+  print_vec("df_adjoint", an);
+  // ---------------------------------------------------------------- 2
+  NumericalCoarseningUsingMultigrid nc;
+  int N[3] = {4, 4, 4};
+  std::vector<BaseMaterial> mats = {{0.1, 0.15}, {1.0 / 2.6, 0.3 / (1.3 * 0.4)}};  // (mu, lambda)
+  nc.init(N, 1, 2, mats, NumericalCoarseningUsingMultigrid::Cubic);
+  std::vector<std::vector<int>> structs(3, std::vector<int>(64));
+  for (auto& s : structs)
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j)
+        for (int k = 0; k < 4; ++k) {   // x<->y symmetric so the cubic relations are meaningful
+          const int a = std::min(i, j), b = std::max(i, j);
+          s[(i * 4 + j) * 4 + k] = ((a * 7 + b * 3 + k * 5 + (int)(&s - &structs[0])) % 3) != 0;
+        }
+  std::vector<double> dens = {0.0, 1.0};
+  std::vector<double> tv, pv, tvb, pvb;
+  for (auto& s : structs)
+    nc.computeCoarsenedElasticityTensorAndParameters3D(s, N, dens, NumericalCoarseningUsingMultigrid::Cubic, tv, pv);
+  nc.computeBatch(structs, N, dens, NumericalCoarseningUsingMultigrid::Cubic, tvb, pvb);
+  double dmax = 0;
+  for (size_t i = 0; i < tv.size(); ++i) dmax = std::fmax(dmax, std::fabs(tv[i] - tvb[i]));
+  if (tv.size() != 63 || pv.size() != 12 || dmax > 1e-9) ++fails;
+  print_vec("coarsened_tensors", tv);
+  print_vec("coarsened_params", pv);
+  std::printf("\"batch_max_diff\": %.3g,\n", dmax);
+  std::vector<double> mat0;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j)
+      for (int k = 0; k < 4; ++k) mat0.push_back(structs[0][(i * 4 + j) * 4 + k]);
+  print_vec("struct0", mat0);
+  // ---------------------------------------------------------------- 3
+  const std::string tmp = "/tmp/femh_level0_elasticityTensors.bin";
+  std::vector<float> tf(tv.begin(), tv.end()), back;
+  std::vector<std::vector<int>> back2;
+  bool ok = writeBinary(tmp, tf) && readBinary(tmp, back) && back == tf;
+  ok = ok && writeBinary(tmp, structs) && readBinary(tmp, back2) && back2 == structs;
+  if (!ok) ++fails;
+  std::printf("\"binary_roundtrip\": %s,\n", ok ? "true" : "false");
+  std::printf("\"fails\": %d\n}\n", fails);
+  return fails ? 1 : 0;
+}

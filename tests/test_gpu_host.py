@@ -1,0 +1,65 @@
+"""GPU test of the reference-facing C++ layer (fem_b200/host): the C++ program
+tests/cpp/test_host.cpp drives FEM3DFun and NumericalCoarseningUsingMultigrid
+like the reference's callers do; its outputs are checked here against the
+oracle and against finite differences."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def host_out(femh, tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("cpp") / "test_host")
+    lib = os.path.join(ROOT, "fem_b200")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-o", exe, os.path.join(ROOT, "tests", "cpp", "test_host.cpp"),
+                    f"-L{lib}", "-lfemh", f"-Wl,-rpath,{lib}"], check=True)
+    res = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stdout + res.stderr
+    return json.loads(res.stdout)
+
+
+def test_fem3dfun_G_matches_oracle(host_out, oracle):
+    n = 8
+    x0 = np.array(host_out["x0"]).reshape(n, n, n)
+    rho = np.clip(x0, 1e-3, 1.0)
+    Co, *_ = oracle.homogenize(rho, mat=oracle.material(interp=oracle.INTERP_RAMP3, E_s=1.0))
+    G = np.array(host_out["G"]).reshape(6, 6)
+    assert np.abs(G - Co).max() < 1e-8 * np.abs(Co).max()
+    assert host_out["density"] == pytest.approx(rho.mean(), rel=1e-12)
+
+
+def test_fem3dfun_df_matches_central_differences(host_out):
+    fd = np.array(host_out["df_fd"])
+    an = np.array(host_out["df_adjoint"])
+    assert np.abs(fd - an).max() <= 1e-5 * np.abs(an).max()
+
+
+def test_coarsening_outputs(host_out, oracle):
+    tv = np.array(host_out["coarsened_tensors"])
+    pv = np.array(host_out["coarsened_params"])
+    assert tv.size == 63 and pv.size == 12 and host_out["batch_max_diff"] < 1e-9
+    # structure 0, replicated once, subdivided twice -> 8^3 cell, two-material law
+    s0 = np.array(host_out["struct0"]).reshape(4, 4, 4)
+    cells = np.repeat(np.repeat(np.repeat(s0, 2, 0), 2, 1), 2, 2)
+    mu1, lam1 = 1.0 / 2.6, 0.3 / (1.3 * 0.4)
+    E1 = mu1 * (3 * lam1 + 2 * mu1) / (lam1 + mu1)
+    nu1 = lam1 / (2 * (lam1 + mu1))
+    mat = oracle.material(interp=oracle.INTERP_BINARY, bin_hi=E1, bin_lo=E1 * 1e-4, nu=nu1)
+    Co, *_ = oracle.homogenize(cells.astype(float), mat=mat)
+    lower = np.array([Co[i, j] for i in range(6) for j in range(i + 1)])
+    assert np.abs(tv[:21] - lower).max() < 1e-8 * np.abs(lower).max()
+    r, E, nu, G = pv[:4]
+    a = Co[0, 1] / Co[0, 0]
+    assert r == pytest.approx(s0.mean(), rel=1e-12)
+    assert nu == pytest.approx(a / (1 + a), rel=1e-8)
+    assert G == pytest.approx(Co[3, 3], rel=1e-8)
+
+
+def test_binary_roundtrip(host_out):
+    assert host_out["binary_roundtrip"] and host_out["fails"] == 0

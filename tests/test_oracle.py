@@ -111,3 +111,18 @@ def test_dCdrho_consistent_with_grad(oracle):
             acc += d[t] * (W[I, I] if I == J else W[I, J] + W[J, I])
             t += 1
     assert np.abs(acc - g).max() < 1e-12 * np.abs(g).max()
+
+
+def test_k0_matches_reference_femlib_code(oracle):
+    """The reference's own femlib element code (compiled from its sources by
+    oracle/build_ref.sh, FP64) gives the same K0 up to its float Gauss points
+    (femlib/src/Quadrature.cpp:3-7): ~1e-8."""
+    import ctypes
+    path = os.path.join(os.path.dirname(os.path.dirname(__file__)), "oracle", "_ref", "libfemlib_ref.so")
+    if not os.path.exists(path):
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    L = ctypes.CDLL(path)
+    for nu in (0.3, 0.45):
+        K = np.zeros((24, 24))
+        assert L.femlib_k0(ctypes.c_double(1.0), ctypes.c_double(nu), K.ctypes.data_as(ctypes.c_void_p)) == 0
+        assert np.abs(K - oracle.k0(1.0, nu, 1.0)).max() < 2e-8
