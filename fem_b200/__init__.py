@@ -5,4 +5,4 @@ include/femh.h); this package is its Python binding and a torch autograd
 wrapper.  See femh.py.
 """
 from .femh import (Config, Engine, FemhError, load_library, LIB_PATH, EXPORTS,  # noqa: F401
-                   INTERP_SIMP, INTERP_RAMP3, INTERP_BINARY, FP64, MIXED, JACOBI_PCG, GMG_PCG)
+                   INTERP_SIMP, INTERP_RAMP3, INTERP_BINARY, FP64, MIXED, MIXED_PC, JACOBI_PCG, GMG_PCG)

@@ -211,6 +211,7 @@ struct Level {
   long long ntot = 0, nodes_smooth = 0;
   int level = 0;
   int NT = 256, maxnz = 1;
+  int nz_spec = 0;   // > 0: every cell of the level has this z extent (specialised kernel)
   UnitList all, smooth;      // all cells / cells that continue to a coarser level
   std::vector<int> su_sb, su_se, nu_sb, nu_se;   // slot ranges per cell (all lists)
   int *d_su_sb = nullptr, *d_su_se = nullptr, *d_nu_sb = nullptr, *d_nu_se = nullptr;
@@ -253,7 +254,7 @@ struct femh_handle {
   // setup cache
   std::vector<int> shape_key;
   std::vector<double> h_key;
-  int prec_key = -1, solver_key = -1;
+  int prec_key = -1, solver_key = -1, bf16_key = -1;
   Arena setup;
   std::vector<Level> levels;
   int ncells = 0;
@@ -369,7 +370,7 @@ void set_err(femh_handle* h, const std::string& m) {
 MatLaw make_law(const femh_config& c) {
   MatLaw m{};
   m.interp = c.interp;
-  m.rho_bf16 = (c.precision == FEMH_MIXED && c.store_bf16) ? 1 : 0;
+  m.rho_bf16 = (c.precision != FEMH_FP64 && c.store_bf16) ? 1 : 0;
   m.E_s = c.E_s;
   m.E_min = c.E_min;
   m.penal = c.penal;
@@ -414,10 +415,10 @@ template <typename T> size_t esize() { return sizeof(T); }
 // ======================================================== kernel launch ===
 namespace {
 
-template <typename T, int NT, int OUT, typename TIn, typename TOut, typename TB, typename TC>
+template <typename T, int NT, int OUT, int NZ, typename TIn, typename TOut, typename TB, typename TC>
 void stencil_go(femh_handle* H, dim3 grid, size_t smem, const StencilArgs<TIn, TOut, TB, TC>& a) {
   static bool attr = false;
-  auto fn = stencil_kernel<T, NT, OUT, TIn, TOut, TB, TC>;
+  auto fn = stencil_kernel<T, NT, OUT, NZ, TIn, TOut, TB, TC>;
   if (!attr) {
     CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     attr = true;
@@ -445,20 +446,42 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   a.ntot = L.ntot;
   a.k = H->hk;
   a.omega = omega;
-  const size_t smem = sizeof(T) * (size_t)(15 * L.NT + 3 * L.maxnz) + 64 * sizeof(double);
+  const size_t smem = 2 * sizeof(T) * (size_t)(15 * L.NT + 3 * L.maxnz) + 16 + 64 * sizeof(double);
   dim3 grid((unsigned)ul.su.size(), kNumRhs);
   static const char* mode_names[] = {"apply", "apply_dot", "jacobi", "jacobi_dot", "resid"};
   char nm[64];
   snprintf(nm, sizeof nm, "stencil_%s_%s_L%d", sizeof(T) == 8 ? "f64" : "f32", mode_names[OUT], L.level);
-  const double nodes = (double)(smooth_only ? L.nodes_smooth : L.ntot);
+  // algorithmic bytes: only (cell, load case) pairs still iterating move data
+  double nodes = 0.0;
+  if (H->prof) {
+    for (const auto& cd : L.cells) {
+      if (smooth_only && cd.child < 0) continue;
+      int act = kNumRhs;
+      if (stt) {
+        act = 0;
+        for (int q = 0; q < kNumRhs; ++q) act += H->state[cd.id * kNumRhs + q].active ? 1 : 0;
+      }
+      nodes += (double)cd.nx * cd.ny * cd.nz * act / kNumRhs;
+    }
+  }
   double per = 18.0 * (sizeof(TIn) + sizeof(TOut)) + sizeof(TC);
   if (OUT >= OUT_JACOBI) per += 18.0 * sizeof(TB) + (OUT == OUT_RESID ? 0.0 : 4.0);
   std::string key(nm);
   Prof prof_(H, H->prof ? H->kstats.emplace(key, femh_handle::KStat{}).first->first.c_str() : nm, nodes * per);
+  switch (L.nz_spec) {   // compile-time z extent (threads fixed per extent)
+    case 16: stencil_go<T, 512, OUT, 16>(H, grid, smem, a); return;
+    case 24: stencil_go<T, 480, OUT, 24>(H, grid, smem, a); return;
+    case 32: stencil_go<T, 512, OUT, 32>(H, grid, smem, a); return;
+    case 48: stencil_go<T, 480, OUT, 48>(H, grid, smem, a); return;
+    case 64: stencil_go<T, 512, OUT, 64>(H, grid, smem, a); return;
+    case 128: stencil_go<T, 512, OUT, 128>(H, grid, smem, a); return;
+    case 256: stencil_go<T, 512, OUT, 256>(H, grid, smem, a); return;
+    default: break;
+  }
   switch (L.NT) {
-    case 128: stencil_go<T, 128, OUT>(H, grid, smem, a); break;
-    case 256: stencil_go<T, 256, OUT>(H, grid, smem, a); break;
-    case 512: stencil_go<T, 512, OUT>(H, grid, smem, a); break;
+    case 128: stencil_go<T, 128, OUT, 0>(H, grid, smem, a); break;
+    case 256: stencil_go<T, 256, OUT, 0>(H, grid, smem, a); break;
+    case 512: stencil_go<T, 512, OUT, 0>(H, grid, smem, a); break;
     default: throw FemhError{FEMH_E_ARG, "unsupported stencil block size"};
   }
 }
@@ -477,7 +500,8 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   const femh_config& c = H->cfg;
   const bool mixed = c.precision == FEMH_MIXED;
   const bool gmg = c.solver == FEMH_GMG_PCG;
-  if (H->shape_key == shapes && H->h_key == hs && H->prec_key == c.precision && H->solver_key == c.solver)
+  if (H->shape_key == shapes && H->h_key == hs && H->prec_key == c.precision && H->solver_key == c.solver &&
+      H->bf16_key == c.store_bf16)
     return;
   H->setup.release();
   H->levels.clear();
@@ -499,8 +523,10 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
     off += H->cell_vox[i];
   }
   H->nvox = off;
-  const size_t vsz = mixed ? sizeof(float) : sizeof(double);
+  const bool mg32 = c.precision != FEMH_FP64;   // multigrid hierarchy in FP32
+  const size_t vsz = mixed ? sizeof(float) : sizeof(double);   // CG vectors
   const size_t psz = mixed ? (c.store_bf16 ? sizeof(__nv_bfloat16) : sizeof(float)) : sizeof(double);
+  const size_t msz = mg32 ? sizeof(float) : sizeof(double);
 
   // ---- levels
   std::vector<std::vector<int>> dims(nc);   // per cell: level dims
@@ -551,6 +577,15 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
     L.NT = std::min(512, std::max(128, pow2ceil(maxrow)));
     if (L.NT < 2 * L.maxnz) L.NT = pow2ceil(2 * L.maxnz);
     if (L.NT > 512) throw FemhError{FEMH_E_ARG, "nz too large for the stencil block"};
+    {
+      bool same = true;
+      for (auto& cd : L.cells) same &= (cd.nz == L.cells[0].nz);
+      const int z0 = L.cells[0].nz;
+      if (same && (z0 == 16 || z0 == 24 || z0 == 32 || z0 == 48 || z0 == 64 || z0 == 128 || z0 == 256)) {
+        L.nz_spec = z0;
+        L.NT = (z0 == 24 || z0 == 48) ? 480 : 512;
+      }
+    }
     int ss = 0, sn = 0;
     for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
       const CellDesc& cd = L.cells[ci];
@@ -581,13 +616,13 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
     L.d_nu_sb = upload(ar, L.nu_sb, s);
     L.d_nu_se = upload(ar, L.nu_se, s);
     // arrays
-    const size_t csz = mixed ? sizeof(float) : sizeof(double);
+    const size_t csz = mg32 ? sizeof(float) : sizeof(double);
     L.kc = ar.get(csz * L.ntot);
     L.invd = ar.arr<float>(L.ntot);
     if (l > 0 || gmg) {
-      L.xa = ar.get(vsz * 18 * L.ntot);
-      L.xb = ar.get(vsz * 18 * L.ntot);
-      if (l > 0) L.bv = ar.get(vsz * 18 * L.ntot);
+      L.xa = ar.get(msz * 18 * L.ntot);
+      L.xb = ar.get(msz * 18 * L.ntot);
+      if (l > 0) L.bv = ar.get(msz * 18 * L.ntot);
     }
     if (!L.coarse_list.empty()) {
       std::vector<long long> aoff;
@@ -623,7 +658,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   H->d_part_s = ar.arr<double>(L0.all.su.size() * kNumRhs);
   H->d_part_n = ar.arr<double>(L0.all.nu.size() * kNumRhs * 2);
   H->d_part_z = ar.arr<double>(L0.all.nu.size() * kNumRhs);
-  H->d_part_e = ar.arr<double>(L0.all.nu.size() * 21);
+  H->d_part_e = ar.arr<double>(L0.all.nu.size() * 22);   // 21 pair energies + sum of rho per slot
   H->d_C = ar.arr<double>(nc * 36);
   H->d_W = ar.arr<double>(nc * 21);
   H->d_out = ar.arr<double>(21 * nv);
@@ -632,6 +667,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   H->h_key = hs;
   H->prec_key = c.precision;
   H->solver_key = c.solver;
+  H->bf16_key = c.store_bf16;
 }
 
 // coefficients on all levels + inverse diagonals + coarse factorisations
@@ -656,7 +692,7 @@ void prepare_operator(femh_handle* H) {
     {
       Prof prof_(H, "k_coarsen_coef", 0.0);
       k_coarsen_coef<TC, TC><<<(unsigned)L.all.nu.size(), 256, 0, s>>>(F.d_cells, L.d_cells, L.all.d_nu,
-                                                                     (const TC*)F.kc, (TC*)L.kc);
+                                                                     (const TC*)F.kc, (TC*)L.kc, c.coarse_avg);
       LAUNCH_CHECK(H);
     }
   }
@@ -701,87 +737,109 @@ bool verbose() {
 
 unsigned fin_blocks(int nc) { return cdiv((long long)nc * kNumRhs * 32, 128); }   // a warp per (cell, rhs)
 
-// One V-cycle of the multigrid preconditioner: z = V(r0).  Level 0's xa must
-// already hold the first damped-Jacobi sweep omega*invd*r0 (written by the CG
-// update kernel).  Buffer roles are fixed by the sweep counts, so the launch
-// sequence is identical every iteration (graph capture).
-template <typename TV, typename TC>
-TV* vcycle(femh_handle* H, const TV* r0) {
+// One V-cycle of the multigrid preconditioner: z = V(r0), levels in TM
+// arithmetic/storage with coefficients TMC; r0 (level-0 right-hand side) may
+// be of another type (FP64 CG residual feeding an FP32 V-cycle).  Level 0's xa
+// must already hold the first damped-Jacobi sweep omega*invd*r0 (written by
+// the CG update kernel).  Buffer roles are fixed by the sweep counts, so the
+// launch sequence is identical every iteration (graph capture).
+template <typename TM, typename TMC, typename TB>
+void vcycle_level_down(femh_handle* H, int l, const TB* b, TM* cur, TM* oth, TM* sol) {
   const femh_config& c = H->cfg;
   cudaStream_t s = H->stream;
   const double om = c.omega;
-  const int nlev = (int)H->levels.size();
   const CGState* stt = H->d_state;
-  std::vector<TV*> sm(nlev), tmp(nlev), sol(nlev);
+  Level& L = H->levels[l];
+  if (!L.coarse_list.empty()) {
+    dim3 g((unsigned)L.coarse_list.size(), kNumRhs);
+    Prof prof_(H, "k_coarse_solve", 0.0);
+    k_coarse_solve<TB, TM><<<g, 256, sizeof(double) * L.coarse_maxm, s>>>(
+        L.d_cells, L.d_coarse_list, L.d_A, L.d_aoff, b, sol, stt, L.ntot);
+    LAUNCH_CHECK(H);
+  }
+  if (L.smooth.su.empty()) return;
+  if (l > 0) {
+    Prof prof_(H, "k_jacobi0", 0.0);
+    k_jacobi0<TB, TM><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, L.smooth.d_nu, b, cur, L.invd, om, stt,
+                                                          L.ntot);
+    LAUNCH_CHECK(H);
+  }
+  for (int sw = 1; sw < c.pre_smooth; ++sw) {
+    stencil<TM, OUT_JACOBI>(H, L, true, (const TM*)cur, oth, b, (const TMC*)L.kc, nullptr, stt, om);
+    std::swap(cur, oth);
+  }
+  stencil<TM, OUT_RESID>(H, L, true, (const TM*)cur, oth, b, (const TMC*)L.kc, nullptr, stt, om);
+  Level& C = H->levels[l + 1];
+  Prof prof_(H, "k_restrict", 0.0);
+  k_restrict<TM, TM><<<NODE_GRID(C.all), 256, 0, s>>>(L.d_cells, C.d_cells, C.all.d_nu, oth, (TM*)C.bv, stt,
+                                                      L.ntot, C.ntot);
+  LAUNCH_CHECK(H);
+}
+
+template <typename TM, typename TMC, typename TB>
+void vcycle_level_up(femh_handle* H, int l, const TB* b, TM* x, TM* t, const TM* coarse_sol) {
+  const femh_config& c = H->cfg;
+  cudaStream_t s = H->stream;
+  const CGState* stt = H->d_state;
+  Level& L = H->levels[l];
+  if (L.smooth.su.empty()) return;
+  Level& C = H->levels[l + 1];
+  {
+    Prof prof_(H, "k_prolong_add", 0.0);
+    k_prolong_add<TM, TM><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, C.d_cells, L.smooth.d_nu, x, coarse_sol,
+                                                              stt, L.ntot, C.ntot);
+    LAUNCH_CHECK(H);
+  }
+  for (int sw = 0; sw < c.post_smooth; ++sw) {
+    stencil<TM, OUT_JACOBI>(H, L, true, (const TM*)x, t, b, (const TMC*)L.kc, nullptr, stt, c.omega);
+    std::swap(x, t);
+  }
+}
+
+template <typename TM, typename TMC, typename TR>
+TM* vcycle(femh_handle* H, const TR* r0) {
+  const femh_config& c = H->cfg;
+  const int nlev = (int)H->levels.size();
+  std::vector<TM*> sm(nlev), tmp(nlev), sol(nlev);
   for (int l = 0; l < nlev; ++l) {
     Level& L = H->levels[l];
-    TV* cur = (TV*)L.xa;
-    TV* oth = (TV*)L.xb;
+    TM* cur = (TM*)L.xa;
+    TM* oth = (TM*)L.xb;
     if ((c.pre_smooth - 1) % 2 == 1) std::swap(cur, oth);   // where the pre-smoothed iterate ends
     sm[l] = cur;
     tmp[l] = oth;
     sol[l] = (c.post_smooth % 2 == 0) ? cur : oth;
   }
   for (int l = 0; l < nlev; ++l) {
-    Level& L = H->levels[l];
-    const TV* b = (l == 0) ? r0 : (const TV*)L.bv;
-    if (!L.coarse_list.empty()) {
-      dim3 g((unsigned)L.coarse_list.size(), kNumRhs);
-      {
-        Prof prof_(H, "k_coarse_solve", 0.0);
-        k_coarse_solve<TV, TV><<<g, 256, sizeof(double) * L.coarse_maxm, s>>>(
-          L.d_cells, L.d_coarse_list, L.d_A, L.d_aoff, b, sol[l], stt, L.ntot);
-        LAUNCH_CHECK(H);
-      }
-    }
-    if (L.smooth.su.empty()) continue;
-    TV* cur = (TV*)L.xa;
-    TV* oth = (TV*)L.xb;
-    if (l > 0) {
-      {
-        Prof prof_(H, "k_jacobi0", 0.0);
-        k_jacobi0<TV, TV><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, L.smooth.d_nu, b, cur, L.invd, om,
-                                                            stt, L.ntot);
-        LAUNCH_CHECK(H);
-      }
-    }
-    for (int sw = 1; sw < c.pre_smooth; ++sw) {
-      stencil<TV, OUT_JACOBI>(H, L, true, (const TV*)cur, oth, b, (const TC*)L.kc, nullptr, stt, om);
-      std::swap(cur, oth);
-    }
-    stencil<TV, OUT_RESID>(H, L, true, (const TV*)cur, oth, b, (const TC*)L.kc, nullptr, stt, om);
-    Level& C = H->levels[l + 1];
-    {
-      Prof prof_(H, "k_restrict", 0.0);
-      k_restrict<TV, TV><<<NODE_GRID(C.all), 256, 0, s>>>(L.d_cells, C.d_cells, C.all.d_nu, oth, (TV*)C.bv, stt,
-                                                        L.ntot, C.ntot);
-      LAUNCH_CHECK(H);
-    }
+    if (l == 0) vcycle_level_down<TM, TMC, TR>(H, 0, r0, (TM*)H->levels[0].xa, (TM*)H->levels[0].xb, sol[0]);
+    else vcycle_level_down<TM, TMC, TM>(H, l, (const TM*)H->levels[l].bv, (TM*)H->levels[l].xa,
+                                         (TM*)H->levels[l].xb, sol[l]);
   }
   for (int l = nlev - 2; l >= 0; --l) {
-    Level& L = H->levels[l];
-    if (L.smooth.su.empty()) continue;
-    Level& C = H->levels[l + 1];
-    const TV* b = (l == 0) ? r0 : (const TV*)L.bv;
-    TV* x = sm[l];
-    TV* t = tmp[l];
-    {
-      Prof prof_(H, "k_prolong_add", 0.0);
-      k_prolong_add<TV, TV><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, C.d_cells, L.smooth.d_nu, x,
-                                                              (const TV*)sol[l + 1], stt, L.ntot, C.ntot);
-      LAUNCH_CHECK(H);
-    }
-    for (int sw = 0; sw < c.post_smooth; ++sw) {
-      stencil<TV, OUT_JACOBI>(H, L, true, (const TV*)x, t, b, (const TC*)L.kc, nullptr, stt, om);
-      std::swap(x, t);
-    }
+    if (l == 0) vcycle_level_up<TM, TMC, TR>(H, 0, r0, sm[0], tmp[0], sol[1]);
+    else vcycle_level_up<TM, TMC, TM>(H, l, (const TM*)H->levels[l].bv, sm[l], tmp[l], sol[l + 1]);
   }
   return sol[0];
 }
 
+// Solver precisions: TV = CG vectors, TP = search direction storage, TK = CG
+// operator coefficients, TM / TMC = multigrid level vectors / coefficients.
+template <typename TV, typename TP, typename TK, typename TM, typename TMC>
+struct Prec {
+  using V = TV;
+  using P = TP;
+  using K = TK;
+  using M = TM;
+  using MC = TMC;
+};
+
 // One PCG iteration (all cells / load cases; inactive ones skip their work).
-template <typename TV, typename TP, typename TC>
-void pcg_iteration(femh_handle* H) {
+template <class PR>
+void pcg_iteration(femh_handle* H, const typename PR::K* kcg) {
+  using TV = typename PR::V;
+  using TP = typename PR::P;
+  using TM = typename PR::M;
+  using TMC = typename PR::MC;
   const femh_config& c = H->cfg;
   cudaStream_t s = H->stream;
   Level& L0 = H->levels[0];
@@ -792,8 +850,7 @@ void pcg_iteration(femh_handle* H) {
   TP* p = (TP*)H->cg_p;
   TV* q = (TV*)H->cg_q;
   CGState* stt = H->d_state;
-  stencil<TV, OUT_APPLY_DOT>(H, L0, false, (const TP*)p, q, (const TV*)nullptr, (const TC*)L0.kc, H->d_part_s,
-                             stt, 0.0);
+  stencil<TV, OUT_APPLY_DOT>(H, L0, false, (const TP*)p, q, (const TV*)nullptr, kcg, H->d_part_s, stt, 0.0);
   {
     Prof prof_(H, "k_fin_alpha", 0.0);
     k_fin_alpha<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_su_sb, L0.d_su_se, H->d_part_s, nc);
@@ -801,37 +858,39 @@ void pcg_iteration(femh_handle* H) {
   }
   {
     Prof prof_(H, "k_cg_update", 0.0);
-    k_cg_update<TV, TP, TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(
-      L0.d_cells, L0.all.d_nu, x, r, p, q, L0.invd, gmg ? (TV*)L0.xa : (TV*)nullptr, c.omega, stt, H->d_part_n,
-      L0.ntot);
+    k_cg_update<TV, TP, TV, TM><<<NODE_GRID(L0.all), 256, 0, s>>>(
+        L0.d_cells, L0.all.d_nu, x, r, p, q, L0.invd, gmg ? (TM*)L0.xa : (TM*)nullptr, c.omega, stt,
+        H->d_part_n, L0.ntot);
     LAUNCH_CHECK(H);
   }
-  TV* z = nullptr;
+  TM* z = nullptr;
   if (gmg) {
-    z = vcycle<TV, TC>(H, r);
-    {
-      Prof prof_(H, "k_dot", 0.0);
-      k_dot<TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
-      LAUNCH_CHECK(H);
-    }
+    z = vcycle<TM, TMC, TV>(H, r);
+    Prof prof_(H, "k_dot", 0.0);
+    k_dot<TM, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
+    LAUNCH_CHECK(H);
   }
   {
     Prof prof_(H, "k_fin_beta", 0.0);
     k_fin_beta<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_n, H->d_part_z, nc,
-                                            gmg ? 0 : 1);
+                                              gmg ? 0 : 1);
     LAUNCH_CHECK(H);
   }
   {
     Prof prof_(H, "k_cg_dir", 0.0);
-    k_cg_dir<TP, TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, p, (const TV*)z,
-                                                         (const TV*)r, L0.invd, stt, L0.ntot);
+    k_cg_dir<TP, TM, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, p, (const TM*)z,
+                                                           (const TV*)r, L0.invd, stt, L0.ntot);
     LAUNCH_CHECK(H);
   }
 }
 
 // PCG on K x = scale*b for every (cell, rhs) whose state is active.
-template <typename TV, typename TP, typename TC, typename TB>
-void pcg(femh_handle* H, const TB* b, int max_iter, double tol, int iters_out[]) {
+template <class PR, typename TB>
+void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, double tol, int iters_out[]) {
+  using TV = typename PR::V;
+  using TP = typename PR::P;
+  using TM = typename PR::M;
+  using TMC = typename PR::MC;
   const femh_config& c = H->cfg;
   cudaStream_t s = H->stream;
   Level& L0 = H->levels[0];
@@ -850,7 +909,7 @@ void pcg(femh_handle* H, const TB* b, int max_iter, double tol, int iters_out[])
   {
     Prof prof_(H, "k_cg_init", 0.0);
     k_cg_init<TB, TV, TP><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, b, x, r, p, L0.invd, stt,
-                                                          H->d_part_n, L0.ntot, gmg ? 0 : 1);
+                                                            H->d_part_n, L0.ntot, gmg ? 0 : 1);
     LAUNCH_CHECK(H);
   }
   {
@@ -861,19 +920,19 @@ void pcg(femh_handle* H, const TB* b, int max_iter, double tol, int iters_out[])
   if (gmg) {
     {
       Prof prof_(H, "k_jacobi0", 0.0);
-      k_jacobi0<TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, r, (TV*)L0.xa, L0.invd,
-                                                        c.omega, stt, L0.ntot);
+      k_jacobi0<TV, TM><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, r, (TM*)L0.xa, L0.invd,
+                                                          c.omega, stt, L0.ntot);
       LAUNCH_CHECK(H);
     }
-    TV* z = vcycle<TV, TC>(H, r);
+    TM* z = vcycle<TM, TMC, TV>(H, r);
     {
       Prof prof_(H, "k_copy", 0.0);
-      k_copy<TP, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, p, z, stt, L0.ntot);
+      k_copy<TP, TM><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, p, z, stt, L0.ntot);
       LAUNCH_CHECK(H);
     }
     {
       Prof prof_(H, "k_dot", 0.0);
-      k_dot<TV, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
+      k_dot<TM, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
       LAUNCH_CHECK(H);
     }
     {
@@ -882,7 +941,7 @@ void pcg(femh_handle* H, const TB* b, int max_iter, double tol, int iters_out[])
       LAUNCH_CHECK(H);
     }
   }
-  const int chunk = std::max(1, c.graph_chunk > 0 ? c.graph_chunk : 8);
+  const int chunk = H->prof ? 1 : std::max(1, c.graph_chunk > 0 ? c.graph_chunk : 8);
   cudaGraphExec_t exec = nullptr;
   long long graph_kernels = 0;
   if (c.graph_chunk > 0 && !H->prof) {
@@ -891,7 +950,7 @@ void pcg(femh_handle* H, const TB* b, int max_iter, double tol, int iters_out[])
     H->cap_count = 0;
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
-      for (int i = 0; i < chunk; ++i) pcg_iteration<TV, TP, TC>(H);
+      for (int i = 0; i < chunk; ++i) pcg_iteration<PR>(H, kcg);
     } catch (...) {
       H->capturing = false;
       cudaStreamEndCapture(s, &g);
@@ -911,7 +970,7 @@ void pcg(femh_handle* H, const TB* b, int max_iter, double tol, int iters_out[])
         CK(cudaGraphLaunch(exec, s));
         H->launches += graph_kernels;
       } else {
-        for (int i = 0; i < chunk; ++i) pcg_iteration<TV, TP, TC>(H);
+        for (int i = 0; i < chunk; ++i) pcg_iteration<PR>(H, kcg);
       }
       done += chunk;
       CK(cudaMemcpyAsync(H->state.data(), stt, sizeof(CGState) * H->state.size(), cudaMemcpyDeviceToHost, s));
@@ -980,18 +1039,22 @@ void solve_all(femh_handle* H, std::vector<femh_solve_info>& infos) {
   CK(cudaEventRecord(H->ev0, s));
   if (c.precision == FEMH_FP64) prepare_operator<double>(H);
   else prepare_operator<float>(H);
+  const float* kc32 = (const float*)L0.kc;
   std::vector<double> bn2;
   norms_of(H, H->b64, bn2);
   std::vector<double> rn2;
   int outer_done = 0;
   std::vector<int> final_status(nc * kNumRhs, CG_CONVERGED);
-  if (c.precision == FEMH_FP64) {
+  if (c.precision == FEMH_FP64 || c.precision == FEMH_MIXED_PC) {
     for (auto& S : H->state) {
       S = CGState{};
       S.active = 1;
       S.scale = 1.0;
     }
-    pcg<double, double, double, double>(H, H->b64, c.max_iter, c.tol, iters.data());
+    if (c.precision == FEMH_FP64)
+      pcg<Prec<double, double, double, double, double>>(H, H->b64, H->kc64, c.max_iter, c.tol, iters.data());
+    else   // FP64 CG and operator, FP32 multigrid preconditioner
+      pcg<Prec<double, double, double, float, float>>(H, H->b64, H->kc64, c.max_iter, c.tol, iters.data());
     for (int t = 0; t < nc * kNumRhs; ++t) final_status[t] = H->state[t].status;
     outer_done = 1;
     true_residual(H, rn2);
@@ -1015,9 +1078,9 @@ void solve_all(femh_handle* H, std::vector<femh_solve_info>& infos) {
       if (!any) break;
       outer_done++;
       if (c.store_bf16)
-        pcg<float, __nv_bfloat16, float, double>(H, H->r64, c.max_iter, c.inner_tol, iters.data());
+        pcg<Prec<float, __nv_bfloat16, float, float, float>>(H, H->r64, kc32, c.max_iter, c.inner_tol, iters.data());
       else
-        pcg<float, float, float, double>(H, H->r64, c.max_iter, c.inner_tol, iters.data());
+        pcg<Prec<float, float, float, float, float>>(H, H->r64, kc32, c.max_iter, c.inner_tol, iters.data());
       for (int t = 0; t < nc * kNumRhs; ++t)
         if (H->state[t].status == CG_BREAKDOWN && H->state[t].iters == 0) outer_on[t] = 0;
       {
@@ -1146,13 +1209,15 @@ void to_host_or_dev(femh_handle* H, double* dst, const double* src, size_t n, in
 void check_config(const femh_config& c) {
   if (c.interp < 0 || c.interp > 2) throw FemhError{FEMH_E_ARG, "interp must be SIMP, RAMP3 or BINARY"};
   if (!(c.nu > -1.0 && c.nu < 0.5)) throw FemhError{FEMH_E_ARG, "nu must lie in (-1, 0.5)"};
-  if (c.precision != FEMH_FP64 && c.precision != FEMH_MIXED) throw FemhError{FEMH_E_ARG, "bad precision"};
+  if (c.precision != FEMH_FP64 && c.precision != FEMH_MIXED && c.precision != FEMH_MIXED_PC)
+    throw FemhError{FEMH_E_ARG, "bad precision"};
   if (c.solver != FEMH_JACOBI_PCG && c.solver != FEMH_GMG_PCG) throw FemhError{FEMH_E_ARG, "bad solver"};
   if (c.solver == FEMH_GMG_PCG && (c.pre_smooth < 1 || c.post_smooth < 0))
     throw FemhError{FEMH_E_ARG, "pre_smooth >= 1 and post_smooth >= 0 are required"};
   if (!(c.tol > 0.0) || c.max_iter < 1) throw FemhError{FEMH_E_ARG, "tol > 0 and max_iter >= 1 are required"};
   if (c.precision == FEMH_MIXED && (!(c.inner_tol > 0.0) || c.max_outer < 1))
     throw FemhError{FEMH_E_ARG, "inner_tol > 0 and max_outer >= 1 are required"};
+  if (c.coarse_avg < 0 || c.coarse_avg > 2) throw FemhError{FEMH_E_ARG, "coarse_avg must be 0, 1 or 2"};
   if (!(c.E_s > 0.0) || c.E_min < 0.0 || !(c.rho_max >= c.rho_min))
     throw FemhError{FEMH_E_ARG, "bad material law parameters"};
 }
@@ -1185,6 +1250,7 @@ femh_status femh_config_default(femh_config* c) {
   c->max_outer = 8;
   c->store_bf16 = 0;
   c->graph_chunk = 8;
+  c->coarse_avg = 0;
   return FEMH_OK;
 }
 

@@ -60,6 +60,7 @@ __global__ void k_coef(const CellDesc* cells, const NodeUnit* units, const doubl
                        double* kc64, TC2* kc2, double* rho_used) {
   const NodeUnit u = units[blockIdx.x];
   const CellDesc cd = cells[u.cell];
+  #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
     double r = rho[cd.off + n];
     r = fmin(fmax(r, law.rho_min), law.rho_max);
@@ -75,22 +76,27 @@ __global__ void k_coef(const CellDesc* cells, const NodeUnit* units, const doubl
   }
 }
 
-// Rediscretised coarse scale: coarse voxel E = mean of its 8 children, voxel
-// edge 2h, so kc_c = (1/8) sum kc_f * 2 = (1/4) sum kc_f.
+// Rediscretised coarse scale: the coarse voxel's modulus is the mean of its 8
+// children's moduli and its edge is 2h, so kc_c = mean(kc_f / h) * 2h =
+// 2 mean(kc_f).  avg: 0 arithmetic mean, 1 geometric, 2 harmonic.
 template <typename TF, typename TCo>
 __global__ void k_coarsen_coef(const CellDesc* fine, const CellDesc* coarse, const NodeUnit* units,
-                               const TF* kcf, TCo* kcc) {
+                               const TF* kcf, TCo* kcc, int avg) {
   const NodeUnit u = units[blockIdx.x];
   const CellDesc cc = coarse[u.cell], cf = fine[cc.parent];
+  #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
     int i, j, k;
     node_ijk(n, cc.ny, cc.nz, i, j, k);
     double s = 0.0;
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
-      s += (double)kcf[cf.off + lin(2 * i + ((a >> 2) & 1), 2 * j + ((a >> 1) & 1), 2 * k + (a & 1),
-                                    cf.ny, cf.nz)];
-    kcc[cc.off + n] = (TCo)(0.25 * s);
+    for (int a = 0; a < 8; ++a) {
+      const double v = (double)kcf[cf.off + lin(2 * i + ((a >> 2) & 1), 2 * j + ((a >> 1) & 1), 2 * k + (a & 1),
+                                                cf.ny, cf.nz)];
+      s += (avg == 0) ? v : (avg == 1 ? log(v) : 1.0 / v);
+    }
+    const double m = (avg == 0) ? s / 8.0 : (avg == 1 ? exp(s / 8.0) : 8.0 / s);
+    kcc[cc.off + n] = (TCo)(2.0 * m);
   }
 }
 
@@ -101,6 +107,7 @@ __global__ void k_invdiag(const CellDesc* cells, const NodeUnit* units, const TC
                           float* invd) {
   const NodeUnit u = units[blockIdx.x];
   const CellDesc cd = cells[u.cell];
+  #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
     int i, j, k;
     node_ijk(n, cd.ny, cd.nz, i, j, k);
@@ -122,6 +129,7 @@ __global__ void k_rhs(const CellDesc* cells, const NodeUnit* units, const double
   const NodeUnit u = units[blockIdx.x];
   const int I = blockIdx.y;
   const CellDesc cd = cells[u.cell];
+  #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
     int i, j, k;
     node_ijk(n, cd.ny, cd.nz, i, j, k);
@@ -144,8 +152,8 @@ __global__ void k_rhs(const CellDesc* cells, const NodeUnit* units, const double
 // With jacobi != 0 also partial r.(invd r) for the Jacobi-preconditioned rz and
 // p = invd r.  Partials: [slot][6][2].
 template <typename TB, typename TV, typename TP>
-__global__ void k_cg_init(const CellDesc* cells, const NodeUnit* units, const TB* b, TV* x, TV* r,
-                          TP* p, const float* invd, const CGState* stt, double* part, long long ntot,
+__global__ void k_cg_init(const CellDesc* cells, const NodeUnit* units, const TB* __restrict__ b, TV* __restrict__ x, TV* __restrict__ r,
+                          TP* __restrict__ p, const float* __restrict__ invd, const CGState* stt, double* __restrict__ part, long long ntot,
                           int jacobi) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
@@ -153,7 +161,8 @@ __global__ void k_cg_init(const CellDesc* cells, const NodeUnit* units, const TB
   const CGState S = stt[cd.id * kNumRhs + rhs];
   double v[2] = {0.0, 0.0};
   if (S.active) {
-    for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+    #pragma unroll 4
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
       const long long g = cd.off + n;
       const float id = invd[g];
 #pragma unroll
@@ -183,9 +192,9 @@ __global__ void k_cg_init(const CellDesc* cells, const NodeUnit* units, const TB
 // Jacobi, r.(invd r).  For the multigrid preconditioner (z0 != nullptr) it
 // also writes the first damped-Jacobi sweep from zero: z0 = omega invd r.
 template <typename TV, typename TP, typename TQ, typename TZ>
-__global__ void k_cg_update(const CellDesc* cells, const NodeUnit* units, TV* x, TV* r, const TP* p,
-                            const TQ* q, const float* invd, TZ* z0, double omega, const CGState* stt,
-                            double* part, long long ntot) {
+__global__ void k_cg_update(const CellDesc* cells, const NodeUnit* units, TV* __restrict__ x, TV* __restrict__ r, const TP* __restrict__ p,
+                            const TQ* __restrict__ q, const float* __restrict__ invd, TZ* __restrict__ z0, double omega, const CGState* stt,
+                            double* __restrict__ part, long long ntot) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cd = cells[u.cell];
@@ -193,7 +202,8 @@ __global__ void k_cg_update(const CellDesc* cells, const NodeUnit* units, TV* x,
   double v[2] = {0.0, 0.0};
   if (S.active) {
     const double al = S.alpha;
-    for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+    #pragma unroll 4
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
       const long long g = cd.off + n;
       const double id = (double)invd[g];
 #pragma unroll
@@ -220,14 +230,15 @@ __global__ void k_cg_update(const CellDesc* cells, const NodeUnit* units, TV* x,
 
 // p = z + beta p, with z = invd r (Jacobi) or z read from zvec (multigrid).
 template <typename TP, typename TZ, typename TR>
-__global__ void k_cg_dir(const CellDesc* cells, const NodeUnit* units, TP* p, const TZ* zvec,
-                         const TR* r, const float* invd, const CGState* stt, long long ntot) {
+__global__ void k_cg_dir(const CellDesc* cells, const NodeUnit* units, TP* __restrict__ p, const TZ* __restrict__ zvec,
+                         const TR* __restrict__ r, const float* __restrict__ invd, const CGState* stt, long long ntot) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cd = cells[u.cell];
   const CGState S = stt[cd.id * kNumRhs + rhs];
   if (!S.active) return;
   const double be = S.beta;
+  #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
     const long long g = cd.off + n;
 #pragma unroll
@@ -339,11 +350,12 @@ __global__ void k_fin_beta(CGState* stt, const int* slot_begin, const int* slot_
 // bc(I) = sum_{d in {-1,0,1}^3} prod_s (1 - |d_s|/2) rf(2I + d); 0 at node 0.
 template <typename TF, typename TCo>
 __global__ void k_restrict(const CellDesc* fine, const CellDesc* coarse, const NodeUnit* units,
-                           const TF* rf, TCo* bc, const CGState* stt, long long ntf, long long ntc) {
+                           const TF* __restrict__ rf, TCo* __restrict__ bc, const CGState* stt, long long ntf, long long ntc) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cc = coarse[u.cell], cf = fine[cc.parent];
   if (stt && !stt[cc.id * kNumRhs + rhs].active) return;
+  #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
     int i, j, k;
     node_ijk(n, cc.ny, cc.nz, i, j, k);
@@ -374,11 +386,12 @@ __global__ void k_restrict(const CellDesc* fine, const CellDesc* coarse, const N
 // Trilinear prolongation and correction: xf(n) += sum_I w(n,I) ec(I).
 template <typename TF, typename TCo>
 __global__ void k_prolong_add(const CellDesc* fine, const CellDesc* coarse, const NodeUnit* units,
-                              TF* xf, const TCo* ec, const CGState* stt, long long ntf, long long ntc) {
+                              TF* __restrict__ xf, const TCo* __restrict__ ec, const CGState* stt, long long ntf, long long ntc) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cf = fine[u.cell], cc = coarse[fine[u.cell].child];
   if (stt && !stt[cf.id * kNumRhs + rhs].active) return;
+  #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
     int i, j, k;
     node_ijk(n, cf.ny, cf.nz, i, j, k);
@@ -406,12 +419,13 @@ __global__ void k_prolong_add(const CellDesc* fine, const CellDesc* coarse, cons
 
 // z = omega * invd * b  (first damped-Jacobi sweep from a zero start)
 template <typename TB, typename TX>
-__global__ void k_jacobi0(const CellDesc* cells, const NodeUnit* units, const TB* b, TX* x,
-                          const float* invd, double omega, const CGState* stt, long long ntot) {
+__global__ void k_jacobi0(const CellDesc* cells, const NodeUnit* units, const TB* __restrict__ b, TX* __restrict__ x,
+                          const float* __restrict__ invd, double omega, const CGState* stt, long long ntot) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cd = cells[u.cell];
   if (stt && !stt[cd.id * kNumRhs + rhs].active) return;
+  #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
     const long long g = cd.off + n;
     const double id = (double)invd[g];
@@ -647,12 +661,13 @@ __global__ void k_energy_fin(const CellDesc* cells, const int* slot_begin, const
 // ------------------------------------------------------- misc vector ops ---
 // dst = src (cast), per load case, over all nodes of the units.
 template <typename TD, typename TS>
-__global__ void k_copy(const CellDesc* cells, const NodeUnit* units, TD* dst, const TS* src,
+__global__ void k_copy(const CellDesc* cells, const NodeUnit* units, TD* __restrict__ dst, const TS* __restrict__ src,
                        const CGState* stt, long long ntot) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cd = cells[u.cell];
   if (stt && !stt[cd.id * kNumRhs + rhs].active) return;
+  #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -663,7 +678,7 @@ __global__ void k_copy(const CellDesc* cells, const NodeUnit* units, TD* dst, co
 
 // Defect correction: x64 += d / scale (d from the inner solve).
 template <typename TD>
-__global__ void k_dc_accum(const CellDesc* cells, const NodeUnit* units, double* x64, const TD* d,
+__global__ void k_dc_accum(const CellDesc* cells, const NodeUnit* units, double* __restrict__ x64, const TD* __restrict__ d,
                            const CGState* stt, long long ntot) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
@@ -671,6 +686,7 @@ __global__ void k_dc_accum(const CellDesc* cells, const NodeUnit* units, double*
   const CGState S = stt[cd.id * kNumRhs + rhs];
   if (!S.outer) return;
   const double inv = 1.0 / S.scale;
+  #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -682,14 +698,15 @@ __global__ void k_dc_accum(const CellDesc* cells, const NodeUnit* units, double*
 
 // Partial a.b per (unit, rhs) into part[slot][6] (stride 1).
 template <typename TA, typename TB2>
-__global__ void k_dot(const CellDesc* cells, const NodeUnit* units, const TA* a, const TB2* b,
-                      const CGState* stt, double* part, long long ntot) {
+__global__ void k_dot(const CellDesc* cells, const NodeUnit* units, const TA* __restrict__ a, const TB2* __restrict__ b,
+                      const CGState* stt, double* __restrict__ part, long long ntot) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cd = cells[u.cell];
   double acc[1] = {0.0};
   if (!stt || stt[cd.id * kNumRhs + rhs].active) {
-    for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x)
+    #pragma unroll 4
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x)
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const long long o = ((long long)rhs * 3 + c) * ntot + cd.off + n;
@@ -703,12 +720,13 @@ __global__ void k_dot(const CellDesc* cells, const NodeUnit* units, const TA* a,
 
 // Partial ||v||^2 per (unit, rhs) into part[slot][6] (stride 1).
 template <typename TV>
-__global__ void k_norm2(const CellDesc* cells, const NodeUnit* units, const TV* v, double* part,
+__global__ void k_norm2(const CellDesc* cells, const NodeUnit* units, const TV* __restrict__ v, double* __restrict__ part,
                         long long ntot) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cd = cells[u.cell];
   double acc[1] = {0.0};
+  #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {

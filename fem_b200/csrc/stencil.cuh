@@ -125,7 +125,14 @@ __device__ __forceinline__ void had_block(T (&w)[3][8], const HadK& K, T s) {
   w[0][0] = (T)0; w[1][0] = (T)0; w[2][0] = (T)0;
 }
 
-template <typename T, int NT, int OUT, typename TIn, typename TOut, typename TB, typename TC>
+// NZ > 0: the cell's z extent is a compile-time constant (all index math
+// folds into immediates); NZ == 0: runtime nz.
+//
+// One barrier per x step: P (node plane) and Q (in-plane corner totals) are
+// double-buffered; at step s a thread publishes node plane ie+1 into P[s&1],
+// transforms voxel ie into Q[s&1], and gathers node plane ie-1 from
+// Q[(s-1)&1], which the previous step completed before this step's barrier.
+template <typename T, int NT, int OUT, int NZ, typename TIn, typename TOut, typename TB, typename TC>
 __global__ void __launch_bounds__(NT, 1)
 stencil_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -133,98 +140,154 @@ stencil_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
   const int rhs = blockIdx.y;
   const CellDesc cd = a.cells[un.cell];
   if (a.stt && !a.stt[cd.id * kNumRhs + rhs].active) return;
-  const int nx = cd.nx, ny = cd.ny, nz = cd.nz;
+  const int nx = cd.nx, ny = cd.ny;
+  const int nz = NZ > 0 ? NZ : cd.nz;
   const int R = NT / nz;                 // thread rows (row 0 = y halo)
   const int tid = threadIdx.x;
-  const int r = tid / nz, z = tid - (tid / nz) * nz;
+  const int r = tid / nz, z = tid - r * nz;
   const bool live = r < R && r <= un.rows;   // rows beyond the tile idle
   const int zp = (z + 1 == nz) ? 0 : z + 1;
   const int zm = (z == 0) ? nz - 1 : z - 1;
-  const int jr = (un.j0 - 1 + r + ny) % ny;            // voxel row / lower node row
+  int jr = un.j0 - 1 + r;                     // voxel row / lower node row
+  if (jr < 0) jr += ny;
+  while (jr >= ny) jr -= ny;
   const int jr1 = (jr + 1 == ny) ? 0 : jr + 1;
-  const bool extra = live && r == un.rows;             // also loads row jr+1
+  const bool extra = live && r == un.rows;    // also loads row jr+1
   const bool owner = live && r >= 1;
 
-  T* P = reinterpret_cast<T*>(smem_raw);               // [(R+1)][3][nz]
-  T* Q = P + (size_t)(R + 1) * 3 * nz;                 // [R][12][nz]
-  double* red = reinterpret_cast<double*>(Q + (size_t)R * 12 * nz);
+  const size_t PS = (size_t)(R + 1) * 3 * nz;   // one P buffer
+  const size_t QS = (size_t)R * 12 * nz;        // one Q buffer
+  T* P = reinterpret_cast<T*>(smem_raw);        // [2][(R+1)][3][nz]
+  T* Q = P + 2 * PS;                            // [2][R][12][nz]
+  double* red = reinterpret_cast<double*>(smem_raw + ((sizeof(T) * (2 * PS + 2 * QS) + 15) & ~(size_t)15));
+  const size_t prow = (size_t)r * 3 * nz, qrow = (size_t)r * 12 * nz;
+  const size_t qup = (size_t)(r > 0 ? r - 1 : 0) * 12 * nz;
 
   const long long st = a.ntot;
-  const TIn* ub = a.u + (long long)rhs * 3 * st + cd.off;
   const long long plane = (long long)ny * nz;
-
-  auto load_row = [&](int ip, int jrow, T (&v)[3]) {
-    const long long o = (long long)ip * plane + (long long)jrow * nz + z;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) v[c] = (T)ld_val(ub + c * st + o);
-  };
+  const long long cellsz = (long long)nx * plane;
+  const TIn* ub = a.u + (long long)rhs * 3 * st + cd.off;
+  const long long col0 = (long long)jr * nz + z, col1 = (long long)jr1 * nz + z;
+  const TC* kcb = a.kc + cd.off + col0;
+  const TB* bb = (OUT >= OUT_JACOBI) ? a.b + (long long)rhs * 3 * st + cd.off + col0 : nullptr;
+  const float* ib = a.invd + cd.off + col0;
+  TOut* obase = a.out + (long long)rhs * 3 * st + cd.off + col0;
 
   T ld0[3] = {0, 0, 0}, ld1[3] = {0, 0, 0};
   T kcv = 0, kc_next = 0;
+  T eb[3] = {0, 0, 0}, eb_next[3] = {0, 0, 0};
+  T eid = 0, eid_next = 0;
   T prev[3][4], carry[3][4];
+  T own[3] = {0, 0, 0}, unode[3] = {0, 0, 0};   // of the node plane gathered next
+  long long pg = 0;                              // offset of that node plane
   double acc = 0.0;
 
-  // prologue: node plane i0-1 -> prev
-  {
-    const int ip = (un.i0 - 1 + nx) % nx;
-    if (live) {
-      load_row(ip, jr, ld0);
-      if (extra) load_row(ip, jr1, ld1);
+  auto adv = [&](long long& o) { o += plane; if (o >= cellsz) o -= cellsz; };
+  auto gather = [&](const T* Qg) {
+    T y[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      y[c] = own[c] + Qg[qrow + (c * 4 + 1) * nz + zm] + Qg[qup + (c * 4 + 2) * nz + z] +
+             Qg[qup + (c * 4 + 3) * nz + zm];
+    TOut* ob = obase + pg;
+    if (OUT == OUT_APPLY || OUT == OUT_APPLY_DOT) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        P[(r * 3 + c) * nz + z] = ld0[c];
-        if (extra) P[((r + 1) * 3 + c) * nz + z] = ld1[c];
+        st_val(ob + c * st, y[c]);
+        if (OUT == OUT_APPLY_DOT) acc += (double)unode[c] * (double)y[c];
       }
-      kc_next = (T)ld_val(a.kc + cd.off + (long long)ip * plane + (long long)jr * nz + z);
-    }
-    __syncthreads();
-    if (live) {
+    } else {
+      const bool pin = (pg + col0 == 0);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        prev[c][0] = P[(r * 3 + c) * nz + z];
-        prev[c][1] = P[(r * 3 + c) * nz + zp];
-        prev[c][2] = P[((r + 1) * 3 + c) * nz + z];
-        prev[c][3] = P[((r + 1) * 3 + c) * nz + zp];
-        carry[c][0] = carry[c][1] = carry[c][2] = carry[c][3] = (T)0;
+        if (OUT == OUT_RESID) {
+          st_val(ob + c * st, pin ? (T)0 : eb[c] - y[c]);
+        } else {
+          const T xv = unode[c] + (T)a.omega * eid * (eb[c] - y[c]);
+          st_val(ob + c * st, xv);
+          if (OUT == OUT_JACOBI_DOT) acc += (double)xv * (double)eb[c];
+        }
       }
-      const int ip1 = (un.i0 + nx) % nx;
-      load_row(ip1, jr, ld0);
-      if (extra) load_row(ip1, jr1, ld1);
     }
-    __syncthreads();
+  };
+
+  // prologue: node plane i0-1 -> prev (through P[1], which step 1 reuses
+  // only after two barriers)
+  long long pk = (long long)((un.i0 - 1 + nx) % nx) * plane;   // voxel plane of kc_next
+  long long pn = pk;                                           // node plane held in ld
+  if (live) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      ld0[c] = (T)ld_val(ub + c * st + pn + col0);
+      if (extra) ld1[c] = (T)ld_val(ub + c * st + pn + col1);
+    }
+    kc_next = (T)ld_val(kcb + pk);
+    T* Pw = P + PS;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Pw[prow + c * nz + z] = ld0[c];
+      if (extra) Pw[prow + (3 + c) * nz + z] = ld1[c];
+    }
+  }
+  __syncthreads();
+  adv(pn);
+  if (live) {
+    const T* Pr = P + PS + prow;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      prev[c][0] = Pr[c * nz + z];
+      prev[c][1] = Pr[c * nz + zp];
+      prev[c][2] = Pr[(3 + c) * nz + z];
+      prev[c][3] = Pr[(3 + c) * nz + zp];
+      carry[c][0] = carry[c][1] = carry[c][2] = carry[c][3] = (T)0;
+      ld0[c] = (T)ld_val(ub + c * st + pn + col0);
+      if (extra) ld1[c] = (T)ld_val(ub + c * st + pn + col1);
+    }
   }
 
   for (int s = 0; s <= un.len; ++s) {
-    const int ie = (un.i0 - 1 + s + nx) % nx;   // voxel plane
+    // voxel plane ie = i0-1+s (offset pe); node plane ie+1 (offset pn) is in ld
+    const long long pe = pk;
+    T* Pb = P + (s & 1) * PS;
+    T* Qb = Q + (s & 1) * QS;
     if (live) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        P[(r * 3 + c) * nz + z] = ld0[c];
-        if (extra) P[((r + 1) * 3 + c) * nz + z] = ld1[c];
+        Pb[prow + c * nz + z] = ld0[c];
+        if (extra) Pb[prow + (3 + c) * nz + z] = ld1[c];
       }
       kcv = kc_next;
       if (s < un.len) {   // prefetch node plane ie+2 and voxel plane ie+1
-        const int ipn = (ie + 2) % nx;
-        load_row(ipn, jr, ld0);
-        if (extra) load_row(ipn, jr1, ld1);
-        const int ien = (ie + 1) % nx;
-        kc_next = (T)ld_val(a.kc + cd.off + (long long)ien * plane + (long long)jr * nz + z);
+        adv(pn);
+        adv(pk);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          ld0[c] = (T)ld_val(ub + c * st + pn + col0);
+          if (extra) ld1[c] = (T)ld_val(ub + c * st + pn + col1);
+        }
+        kc_next = (T)ld_val(kcb + pk);
+      }
+      if (OUT >= OUT_JACOBI && owner && s >= 1) {   // epilogue operands of node plane ie
+#pragma unroll
+        for (int c = 0; c < 3; ++c) eb_next[c] = (T)ld_val(bb + c * st + pe);
+        if (OUT != OUT_RESID) eid_next = (T)ib[pe];
       }
     }
-    __syncthreads();   // P holds node plane ie+1
-    T own[3] = {0, 0, 0};   // voxel column (jr, z)'s total at node (ie, jr, z)
-    T unode[3] = {0, 0, 0}; // u(ie, jr, z)
+    __syncthreads();   // P[s&1] holds node plane ie+1; Q[(s-1)&1] holds node plane ie-1
+    // gather node plane ie-1 (owned planes i0..i0+len-1 -> steps 2..len+1)
+    if (s >= 2 && owner) gather(Q + ((s - 1) & 1) * QS);
     if (live) {
       T w[3][8];
+      const T* Pr = Pb + prow;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const T c0 = P[(r * 3 + c) * nz + z];
-        const T c1 = P[(r * 3 + c) * nz + zp];
-        const T c2 = P[((r + 1) * 3 + c) * nz + z];
-        const T c3 = P[((r + 1) * 3 + c) * nz + zp];
+        const T c0 = Pr[c * nz + z];
+        const T c1 = Pr[c * nz + zp];
+        const T c2 = Pr[(3 + c) * nz + z];
+        const T c3 = Pr[(3 + c) * nz + zp];
         w[c][0] = prev[c][0]; w[c][1] = prev[c][1]; w[c][2] = prev[c][2]; w[c][3] = prev[c][3];
         w[c][4] = c0; w[c][5] = c1; w[c][6] = c2; w[c][7] = c3;
-        unode[c] = prev[c][0];
+        unode[c] = prev[c][0];      // u at node (ie, jr, z), gathered at the next step
         prev[c][0] = c0; prev[c][1] = c1; prev[c][2] = c2; prev[c][3] = c3;
         fwht8_fwd(w[c]);
       }
@@ -237,43 +300,17 @@ stencil_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
           const T tot = w[c][q] + carry[c][q];
           carry[c][q] = w[c][4 + q];
           if (q == 0) own[c] = tot;
-          else if (s > 0) Q[(r * 12 + c * 4 + q) * nz + z] = tot;
+          else if (s > 0) Qb[qrow + (c * 4 + q) * nz + z] = tot;
         }
       }
-    }
-    __syncthreads();   // Q holds the in-plane corner totals of voxel plane ie
-    if (s > 0 && owner) {
-      const long long node = (long long)ie * plane + (long long)jr * nz + z;
-      T y[3];
+      pg = pe;
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        y[c] = own[c] + Q[(r * 12 + c * 4 + 1) * nz + zm] + Q[((r - 1) * 12 + c * 4 + 2) * nz + z] +
-               Q[((r - 1) * 12 + c * 4 + 3) * nz + zm];
-      TOut* ob = a.out + (long long)rhs * 3 * st + cd.off + node;
-      if (OUT == OUT_APPLY || OUT == OUT_APPLY_DOT) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          st_val(ob + c * st, y[c]);
-          if (OUT == OUT_APPLY_DOT) acc += (double)unode[c] * (double)y[c];
-        }
-      } else {
-        const TB* bb = a.b + (long long)rhs * 3 * st + cd.off + node;
-        const T id = (T)a.invd[cd.off + node];
-        const bool pin = (node == 0);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const T bv = (T)ld_val(bb + c * st);
-          if (OUT == OUT_RESID) {
-            st_val(ob + c * st, pin ? (T)0 : bv - y[c]);
-          } else {
-            const T xv = unode[c] + (T)a.omega * id * (bv - y[c]);
-            st_val(ob + c * st, xv);
-            if (OUT == OUT_JACOBI_DOT) acc += (double)xv * (double)bv;
-          }
-        }
-      }
+      for (int c = 0; c < 3; ++c) eb[c] = eb_next[c];
+      eid = eid_next;
     }
   }
+  __syncthreads();   // Q[len&1] holds the last owned node plane
+  if (un.len >= 1 && owner) gather(Q + (un.len & 1) * QS);
 
   if (OUT == OUT_APPLY_DOT || OUT == OUT_JACOBI_DOT) {
     double v[1] = {acc};
@@ -282,11 +319,12 @@ stencil_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
   }
 }
 
-// Shared memory bytes of one CTA.
+// Shared memory bytes of one CTA (both buffers, + reduction scratch).
 template <typename T>
 inline size_t stencil_smem_bytes(int NT, int nz) {
   const int R = NT / nz;
-  return sizeof(T) * ((size_t)(R + 1) * 3 * nz + (size_t)R * 12 * nz) + 32 * sizeof(double);
+  return ((sizeof(T) * 2 * ((size_t)(R + 1) * 3 * nz + (size_t)R * 12 * nz) + 15) & ~(size_t)15) +
+         32 * sizeof(double);
 }
 
 }  // namespace femh

@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(_HERE, "libfemh.so")
 
 FEMH_OK, FEMH_E_ARG, FEMH_E_CUDA, FEMH_E_OOM, FEMH_E_NOT_CONVERGED, FEMH_E_BREAKDOWN, FEMH_E_STATE = range(7)
 INTERP_SIMP, INTERP_RAMP3, INTERP_BINARY = 0, 1, 2
-FP64, MIXED = 0, 1
+FP64, MIXED, MIXED_PC = 0, 1, 2
 JACOBI_PCG, GMG_PCG = 0, 1
 
 #: every exported symbol of include/femh.h
@@ -52,7 +52,7 @@ class _Config(ctypes.Structure):
         ("omega", ctypes.c_double), ("coarse_max_nodes", ctypes.c_int),
         ("tol", ctypes.c_double), ("max_iter", ctypes.c_int),
         ("inner_tol", ctypes.c_double), ("max_outer", ctypes.c_int),
-        ("store_bf16", ctypes.c_int), ("graph_chunk", ctypes.c_int),
+        ("store_bf16", ctypes.c_int), ("graph_chunk", ctypes.c_int), ("coarse_avg", ctypes.c_int),
     ]
 
 
@@ -130,6 +130,7 @@ class Config:
     max_outer: int = 8
     store_bf16: int = 0
     graph_chunk: int = 8
+    coarse_avg: int = 0
 
     def to_c(self) -> _Config:
         c = _Config()

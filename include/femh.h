@@ -55,7 +55,8 @@ enum { FEMH_INTERP_SIMP = 0,    /* E_min + rho^p (E_s - E_min)   (BASELINE law) 
        FEMH_INTERP_BINARY = 2   /* rho>=0.5 ? bin_hi : bin_lo
                                    NumericalCoarseningUsingMultiGrid.cpp:235-241 */ };
 enum { FEMH_FP64 = 0,           /* plain method, all FP64 */
-       FEMH_MIXED = 1 };        /* FP32 inner solve in FP64 defect correction */
+       FEMH_MIXED = 1,          /* FP32 inner PCG solves in FP64 defect correction */
+       FEMH_MIXED_PC = 2 };     /* FP64 CG + operator, FP32 multigrid preconditioner */
 enum { FEMH_JACOBI_PCG = 0, FEMH_GMG_PCG = 1 };
 
 typedef struct {
@@ -75,6 +76,8 @@ typedef struct {
   int max_outer;          /* mixed: defect-correction steps */
   int store_bf16;         /* mixed: bf16 storage of search directions and rho */
   int graph_chunk;        /* CG iterations per captured CUDA graph (0 = no graphs) */
+  int coarse_avg;         /* coarse voxel modulus from its 8 children: 0 arithmetic mean
+                             (rediscretisation of the mean), 1 geometric, 2 harmonic */
 } femh_config;
 
 typedef struct {
