@@ -13,6 +13,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1549,3 +1550,140 @@ femh_status femh_profile_read(femh_handle* H, femh_kernel_stat* out, int max, in
 }
 
 }  // extern "C"
+
+// ============================================= allocation-free energy entry ===
+// femh_energy_noalloc: C^H of one cell from a caller-provided density and
+// periodic fluctuation, for callers that cannot call cudaMalloc.  Its per-CTA
+// partial sums live in the file-scope device array below instead of in
+// handle-owned memory.
+namespace {
+
+constexpr int kNoAllocSlots = 2048;                          // CTAs of the partial pass
+constexpr long long kNoAllocMaxVoxels = 256LL * 256 * 256;   // largest accepted cell
+// 2048 slots x 21 doubles = 336 KiB on every device that loads the library.
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocSlots * 21];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[256] = {};   // device address of g_noalloc_scratch, per device
+
+// Per voxel u^I = ue0^I(h) + chi^I with chi in the [6][node][3] layout of
+// femh_fluctuation; slot sums of kc_e u^I.K0(1) u^J (21 pairs) into part.
+__global__ void __launch_bounds__(128)
+k_energy_noalloc_partial(int nx, int ny, int nz, double h, const double* __restrict__ rho,
+                         const double* __restrict__ chi, MatLaw law, HadK K, ElemConst ec,
+                         double* __restrict__ part, long long per) {
+  const long long nv = (long long)nx * ny * nz;
+  const long long b = (long long)blockIdx.x * per, e_end = min(nv, b + per);
+  double acc[21];
+#pragma unroll
+  for (int t = 0; t < 21; ++t) acc[t] = 0.0;
+  for (long long e = b + threadIdx.x; e < e_end; e += blockDim.x) {
+    int i, j, k;
+    node_ijk(e, ny, nz, i, j, k);
+    long long nd[8];
+#pragma unroll
+    for (int a8 = 0; a8 < 8; ++a8)
+      nd[a8] = lin(wrap(i + ((a8 >> 2) & 1), nx), wrap(j + ((a8 >> 1) & 1), ny), wrap(k + (a8 & 1), nz), ny, nz);
+    double uh[kNumRhs][3][8];
+#pragma unroll
+    for (int I = 0; I < kNumRhs; ++I)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+#pragma unroll
+        for (int a8 = 0; a8 < 8; ++a8) uh[I][c][a8] = chi[((long long)I * nv + nd[a8]) * 3 + c];
+        fwht8_fwd(uh[I][c]);
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) uh[I][c][kk] += h * ec.uhat0[I][c][kk];
+      }
+    double r = fmin(fmax(rho[e], law.rho_min), law.rho_max);
+    const double ke = law_coef(law, r) * h;
+#pragma unroll
+    for (int J = 0; J < kNumRhs; ++J) {
+      double w[3][8];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) w[c][kk] = uh[J][c][kk];
+      had_block(w, K, 1.0);
+#pragma unroll
+      for (int I = J; I < kNumRhs; ++I) {
+        double d = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int kk = 1; kk < 8; ++kk) d += uh[I][c][kk] * w[c][kk];
+        acc[I * (I + 1) / 2 + J] += ke * d;
+      }
+    }
+  }
+  __shared__ double red[32 * 21];
+  block_reduce<21>(acc, red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int t = 0; t < 21; ++t) part[(long long)blockIdx.x * 21 + t] = acc[t];
+}
+
+// C (6x6, both triangles) from the slot sums, fixed summation order.
+__global__ void k_energy_noalloc_final(double vol, const double* __restrict__ part, int nslots,
+                                       double* __restrict__ C) {
+  const int q = threadIdx.x;
+  if (q >= 21) return;
+  double s = 0.0;
+  for (int sl = 0; sl < nslots; ++sl) s += part[(long long)sl * 21 + q];
+  int I = 0;
+  while ((I + 1) * (I + 2) / 2 <= q) ++I;
+  const int J = q - I * (I + 1) / 2;
+  C[I * 6 + J] = s / vol;
+  C[J * 6 + I] = s / vol;
+}
+
+}  // namespace
+
+extern "C" femh_status femh_energy_noalloc(const femh_config* cfg, int nx, int ny, int nz, double hvox,
+                                           const double* rho, const double* chi, double* C_out,
+                                           void* stream) {
+  if (!cfg || !rho || !chi || !C_out) return FEMH_E_ARG;
+  if (nx < 2 || ny < 2 || nz < 2 || !(hvox > 0.0)) return FEMH_E_ARG;
+  const long long nv = (long long)nx * ny * nz;
+  if (nv > kNoAllocMaxVoxels) return FEMH_E_ARG;   // beyond the scratch array's design limit
+  try {
+    check_config(*cfg);
+  } catch (const FemhError&) {
+    return FEMH_E_ARG;
+  }
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return FEMH_E_CUDA;
+  if (dev != cfg->device) return FEMH_E_ARG;   // runs on the caller's current device only
+  double* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      // set-up, once per device: the host-side symbol is only a stand-in; its
+      // device address must be looked up with the device current
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return FEMH_E_CUDA;
+      g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    scratch = g_noalloc_addr[dev];
+  }
+  double K[576];
+  host_k0(cfg->nu, K);
+  HadK hk;
+  try {
+    hk = host_hadk(K);
+  } catch (const FemhError&) {
+    return FEMH_E_ARG;
+  }
+  const ElemConst ec = host_elemconst(K);
+  MatLaw law = make_law(*cfg);
+  law.rho_bf16 = 0;
+  const long long per = (nv + kNoAllocSlots - 1) / kNoAllocSlots;
+  const int nslots = (int)((nv + per - 1) / per);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  k_energy_noalloc_partial<<<nslots, 128, 0, s>>>(nx, ny, nz, hvox, rho, chi, law, hk, ec, scratch, per);
+  if (cudaGetLastError() != cudaSuccess) return FEMH_E_CUDA;
+  const double vol = (double)nv * hvox * hvox * hvox;
+  k_energy_noalloc_final<<<1, 32, 0, s>>>(vol, scratch, nslots, C_out);
+  if (cudaGetLastError() != cudaSuccess) return FEMH_E_CUDA;
+  return FEMH_OK;
+}

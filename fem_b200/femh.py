@@ -32,6 +32,7 @@ EXPORTS = (
     "femh_config_default", "femh_create", "femh_destroy", "femh_homogenize", "femh_homogenize_grad",
     "femh_dCdrho", "femh_full_field", "femh_fluctuation", "femh_apply_operator", "femh_homogenize_batch",
     "femh_last_error", "femh_set_stream", "femh_kernel_launches", "femh_profile", "femh_profile_read",
+    "femh_energy_noalloc",
 )
 
 
@@ -101,6 +102,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.femh_kernel_launches.restype = ctypes.c_longlong
     L.femh_profile.argtypes = [vp, ip]
     L.femh_profile_read.argtypes = [vp, ctypes.POINTER(_KStat), ip, ctypes.POINTER(ctypes.c_int)]
+    L.femh_energy_noalloc.argtypes = [ctypes.POINTER(_Config), ip, ip, ip, ctypes.c_double, vp, vp, vp, vp]
     _lib = L
     return L
 

@@ -169,6 +169,30 @@ typedef struct {
 femh_status femh_profile(femh_handle* h, int enable);   /* also clears the stats */
 femh_status femh_profile_read(femh_handle* h, femh_kernel_stat* out, int max, int* n);
 
+/* C^H of one cell from a caller-provided density field and periodic
+ * fluctuation, allocating nothing.  No counterpart in the reference: it exists
+ * for callers that cannot call cudaMalloc -- code whose device memory belongs
+ * to another allocator (a host framework's caching allocator that has already
+ * reserved the device, an application that must keep its footprint fixed after
+ * start-up) and latency-critical loops that cannot afford cudaMalloc/cudaFree's
+ * implicit device synchronisation.
+ *   cfg  material law (interp, E_s, E_min, penal, nu, bin_hi/lo, rho clamp);
+ *        cfg->device must be the calling thread's current device
+ *   rho  device pointer, nx*ny*nz densities;   chi  device pointer, the
+ *        fluctuation in femh_fluctuation's layout [6][nx*ny*nz][3]
+ *   C_out device pointer, 36 doubles (6x6 row major, both triangles written)
+ *   stream cudaStream_t as void* (NULL = default stream); the call is
+ *        asynchronous on it.
+ * Limits: nx*ny*nz <= 256^3 (16,777,216 voxels); larger cells return
+ * FEMH_E_ARG before any device work.  Its scratch is a fixed 336 KiB device
+ * array (2048 slots x 21 doubles) that every GPU loading this library holds
+ * until the process exits; every call overwrites it, so calls that overlap on
+ * the GPU (different streams or threads) race -- serialise them.  The first call
+ * on a device looks up that array's device address (cudaGetSymbolAddress) and
+ * caches it; make that first call before any stream capture. */
+femh_status femh_energy_noalloc(const femh_config* cfg, int nx, int ny, int nz, double hvox,
+                                const double* rho, const double* chi, double* C_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
