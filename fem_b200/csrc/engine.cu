@@ -213,6 +213,7 @@ struct Level {
   int level = 0;
   int NT = 256, maxnz = 1;
   int nz_spec = 0;   // > 0: every cell of the level has this z extent (specialised kernel)
+  int chunk = 0;     // x-chunk length of the stencil units (0 = heuristic), set by the autotuner
   UnitList all, smooth;      // all cells / cells that continue to a coarser level
   std::vector<int> su_sb, su_se, nu_sb, nu_se;   // slot ranges per cell (all lists)
   int *d_su_sb = nullptr, *d_su_se = nullptr, *d_nu_sb = nullptr, *d_nu_se = nullptr;
@@ -258,6 +259,7 @@ struct femh_handle {
   int prec_key = -1, solver_key = -1, bf16_key = -1;
   Arena setup;
   std::vector<Level> levels;
+  std::map<std::string, int> tune_cache;   // autotuned x-chunk per level signature
   int ncells = 0;
   std::vector<long long> cell_vox;   // voxels per cell
   std::vector<long long> cell_off;   // fine offsets
@@ -384,11 +386,12 @@ MatLaw make_law(const femh_config& c) {
 
 // Stencil work units of one cell: tiles of up to R-1 rows, x-chunks of len.
 void add_stencil_units(std::vector<StencilUnit>& out, int cellidx, const CellDesc& cd, int NT,
-                       int& slot) {
+                       int& slot, int chunk_req = 0) {
   const int R = NT / cd.nz;
   const int maxrows = std::max(1, std::min(R - 1, cd.ny));
   const int ntiles = (cd.ny + maxrows - 1) / maxrows;
-  const int chunk = cd.nx >= 64 ? 16 : (cd.nx >= 16 ? 8 : cd.nx);
+  const int chunk = chunk_req > 0 ? std::min(chunk_req, cd.nx)
+                                  : (cd.nx >= 128 ? 32 : (cd.nx >= 64 ? 16 : (cd.nx >= 16 ? 8 : cd.nx)));
   const int nchunks = (cd.nx + chunk - 1) / chunk;
   int j = 0;
   for (int t = 0; t < ntiles; ++t) {
@@ -496,6 +499,9 @@ inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) /
 
 // ====================================================== setup / solve ===
 namespace {
+
+template <typename T>
+void autotune_levels(femh_handle* H, bool mg);
 
 void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vector<double>& hs) {
   const femh_config& c = H->cfg;
@@ -655,6 +661,10 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   H->cg_q = ar.get(vsz * 18 * nv);
   H->d_state = ar.arr<CGState>(nc * kNumRhs);
   H->state.assign(nc * kNumRhs, CGState{});
+  if (c.autotune) {
+    if (mg32 || (mixed && !gmg)) autotune_levels<float>(H, gmg);
+    else autotune_levels<double>(H, gmg);
+  }
   const Level& L0 = H->levels[0];
   H->d_part_s = ar.arr<double>(L0.all.su.size() * kNumRhs);
   H->d_part_n = ar.arr<double>(L0.all.nu.size() * kNumRhs * 2);
@@ -669,6 +679,98 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   H->prec_key = c.precision;
   H->solver_key = c.solver;
   H->bf16_key = c.store_bf16;
+}
+
+
+bool verbose() {
+  static const int v = [] {
+    const char* e = std::getenv("FEMH_VERBOSE");
+    return (e && *e && *e != '0') ? 1 : 0;
+  }();
+  return v != 0;
+}
+
+// (Re)build a level's stencil unit lists for an x-chunk length.
+void build_stencil_units(femh_handle* H, Level& L, int chunk) {
+  L.chunk = chunk;
+  L.all.su.clear();
+  L.smooth.su.clear();
+  L.su_sb.clear();
+  L.su_se.clear();
+  int ss = 0;
+  for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
+    L.su_sb.push_back(ss);
+    add_stencil_units(L.all.su, ci, L.cells[ci], L.NT, ss, chunk);
+    L.su_se.push_back(ss);
+  }
+  for (auto& u : L.all.su)
+    if (L.cells[u.cell].child >= 0) L.smooth.su.push_back(u);
+  cudaStream_t s = H->stream;
+  Arena& ar = H->setup;
+  L.all.d_su = upload(ar, L.all.su, s);
+  L.smooth.d_su = upload(ar, L.smooth.su, s);
+  L.d_su_sb = upload(ar, L.su_sb, s);
+  L.d_su_se = upload(ar, L.su_se, s);
+}
+
+// Project autotuner for the stencil's tile shape: for every level whose
+// stencil runs, time the damped-Jacobi sweep (the most launched mode) for
+// x-chunk lengths {4, 8, 16, 32, 64, whole cell} on the level's own buffers
+// and keep the fastest.  Results are cached per level signature in the handle.
+template <typename T>
+void autotune_levels(femh_handle* H, bool mg) {
+  cudaStream_t s = H->stream;
+  for (size_t l = 0; l < H->levels.size(); ++l) {
+    Level& L = H->levels[l];
+    const bool smooth = mg && l > 0;   // coarse levels only run smoothing sweeps
+    if ((smooth ? L.smooth.su : L.all.su).empty()) continue;
+    std::string key = std::to_string(l) + ":" + std::to_string(L.NT) + ":" + std::to_string(sizeof(T));
+    int maxnx = 1;
+    for (auto& cd : L.cells) {
+      key += ":" + std::to_string(cd.nx) + "x" + std::to_string(cd.ny) + "x" + std::to_string(cd.nz);
+      maxnx = std::max(maxnx, cd.nx);
+    }
+    auto it = H->tune_cache.find(key);
+    if (it != H->tune_cache.end()) {
+      if (it->second != L.chunk) build_stencil_units(H, L, it->second);
+      continue;
+    }
+    if (L.ntot < 4096) {   // tiny levels: launch-bound, the heuristic is fine
+      H->tune_cache[key] = L.chunk;
+      continue;
+    }
+    T* in = (T*)(L.xa ? L.xa : H->cg_r);
+    T* out = (T*)(L.xb ? L.xb : H->cg_q);
+    CK(cudaMemsetAsync(L.kc, 0, sizeof(T) * L.ntot, s));
+    CK(cudaMemsetAsync(L.invd, 0, sizeof(float) * L.ntot, s));
+    CK(cudaMemsetAsync(in, 0, sizeof(T) * 18 * L.ntot, s));
+    int best = L.chunk;
+    float best_ms = 1e30f;
+    std::vector<int> cands;
+    for (int cand : {4, 8, 16, 32, 64, maxnx})
+      if (cand <= maxnx && std::find(cands.begin(), cands.end(), cand) == cands.end()) cands.push_back(cand);
+    for (int cand : cands) {
+      build_stencil_units(H, L, cand);
+      float ms_min = 1e30f;
+      for (int rep = 0; rep < 3; ++rep) {
+        CK(cudaEventRecord(H->ev0, s));
+        stencil<T, OUT_JACOBI>(H, L, smooth, (const T*)in, out, (const T*)in, (const T*)L.kc, nullptr, nullptr,
+                               0.5);
+        CK(cudaEventRecord(H->ev1, s));
+        CK(cudaEventSynchronize(H->ev1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, H->ev0, H->ev1));
+        ms_min = std::min(ms_min, ms);
+      }
+      if (verbose()) std::fprintf(stderr, "[femh] tune level %zu chunk %d: %.4f ms\n", l, cand, ms_min);
+      if (ms_min < best_ms) {
+        best_ms = ms_min;
+        best = cand;
+      }
+    }
+    build_stencil_units(H, L, best);
+    H->tune_cache[key] = best;
+  }
 }
 
 // coefficients on all levels + inverse diagonals + coarse factorisations
@@ -727,14 +829,6 @@ void prepare_operator(femh_handle* H) {
   }
 }
 
-
-bool verbose() {
-  static const int v = [] {
-    const char* e = std::getenv("FEMH_VERBOSE");
-    return (e && *e && *e != '0') ? 1 : 0;
-  }();
-  return v != 0;
-}
 
 unsigned fin_blocks(int nc) { return cdiv((long long)nc * kNumRhs * 32, 128); }   // a warp per (cell, rhs)
 
@@ -1252,6 +1346,7 @@ femh_status femh_config_default(femh_config* c) {
   c->store_bf16 = 0;
   c->graph_chunk = 8;
   c->coarse_avg = 0;
+  c->autotune = 1;
   return FEMH_OK;
 }
 

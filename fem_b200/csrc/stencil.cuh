@@ -175,8 +175,8 @@ stencil_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
 
   T ld0[3] = {0, 0, 0}, ld1[3] = {0, 0, 0};
   T kcv = 0, kc_next = 0;
-  T eb[3] = {0, 0, 0}, eb_next[3] = {0, 0, 0};
-  T eid = 0, eid_next = 0;
+  T eb[3] = {0, 0, 0};
+  T eid = 0;
   T prev[3][4], carry[3][4];
   T own[3] = {0, 0, 0}, unode[3] = {0, 0, 0};   // of the node plane gathered next
   long long pg = 0;                              // offset of that node plane
@@ -267,15 +267,17 @@ stencil_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
         }
         kc_next = (T)ld_val(kcb + pk);
       }
-      if (OUT >= OUT_JACOBI && owner && s >= 1) {   // epilogue operands of node plane ie
-#pragma unroll
-        for (int c = 0; c < 3; ++c) eb_next[c] = (T)ld_val(bb + c * st + pe);
-        if (OUT != OUT_RESID) eid_next = (T)ib[pe];
-      }
     }
     __syncthreads();   // P[s&1] holds node plane ie+1; Q[(s-1)&1] holds node plane ie-1
     // gather node plane ie-1 (owned planes i0..i0+len-1 -> steps 2..len+1)
     if (s >= 2 && owner) gather(Q + ((s - 1) & 1) * QS);
+    if (OUT >= OUT_JACOBI && owner && s >= 1) {
+      // epilogue operands of node plane ie, used by the next step's gather:
+      // loaded straight into their registers, a whole step ahead of use
+#pragma unroll
+      for (int c = 0; c < 3; ++c) eb[c] = (T)ld_val(bb + c * st + pe);
+      if (OUT != OUT_RESID) eid = (T)ib[pe];
+    }
     if (live) {
       T w[3][8];
       const T* Pr = Pb + prow;
@@ -304,9 +306,6 @@ stencil_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
         }
       }
       pg = pe;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) eb[c] = eb_next[c];
-      eid = eid_next;
     }
   }
   __syncthreads();   // Q[len&1] holds the last owned node plane

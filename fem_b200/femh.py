@@ -54,6 +54,7 @@ class _Config(ctypes.Structure):
         ("tol", ctypes.c_double), ("max_iter", ctypes.c_int),
         ("inner_tol", ctypes.c_double), ("max_outer", ctypes.c_int),
         ("store_bf16", ctypes.c_int), ("graph_chunk", ctypes.c_int), ("coarse_avg", ctypes.c_int),
+        ("autotune", ctypes.c_int),
     ]
 
 
@@ -133,6 +134,7 @@ class Config:
     store_bf16: int = 0
     graph_chunk: int = 8
     coarse_avg: int = 0
+    autotune: int = 1
 
     def to_c(self) -> _Config:
         c = _Config()

@@ -78,6 +78,7 @@ typedef struct {
   int graph_chunk;        /* CG iterations per captured CUDA graph (0 = no graphs) */
   int coarse_avg;         /* coarse voxel modulus from its 8 children: 0 arithmetic mean
                              (rediscretisation of the mean), 1 geometric, 2 harmonic */
+  int autotune;           /* 1: time the stencil's x-chunk length per level at set-up */
 } femh_config;
 
 typedef struct {
