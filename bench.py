@@ -162,6 +162,7 @@ def main():
     from fem_b200 import build
     build.build()
     import fem_b200 as F
+    from fem_b200.dist import max_over_ranks
 
     n = args.n
     rho_h = fields.smooth_cell(n, 4.0, seed=2 + rank)
@@ -194,11 +195,7 @@ def main():
         e1.record(stream)
         torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1), device="cuda")
         barrier()
         return ms
 

@@ -214,6 +214,16 @@ struct Level {
   int NT = 256, maxnz = 1;
   int nz_spec = 0;   // > 0: every cell of the level has this z extent (specialised kernel)
   int chunk = 0;     // x-chunk length of the stencil units (0 = heuristic), set by the autotuner
+  int variant = 2;   // stencil kernel: 2 = two voxel rows per thread, 1 = one row per thread
+  // level 0 of the mixed modes also runs FP64 operator applies (CG / true
+  // residual): they get their own tuned layout (FP64 kernels spill in the
+  // layout that suits FP32)
+  bool use64 = false;
+  int variant64 = 1, chunk64 = 0;
+  std::vector<StencilUnit> su64;
+  StencilUnit* d_su64 = nullptr;
+  std::vector<int> su64_sb, su64_se;
+  int *d_su64_sb = nullptr, *d_su64_se = nullptr;
   UnitList all, smooth;      // all cells / cells that continue to a coarser level
   std::vector<int> su_sb, su_se, nu_sb, nu_se;   // slot ranges per cell (all lists)
   int *d_su_sb = nullptr, *d_su_se = nullptr, *d_nu_sb = nullptr, *d_nu_se = nullptr;
@@ -386,9 +396,9 @@ MatLaw make_law(const femh_config& c) {
 
 // Stencil work units of one cell: tiles of up to R-1 rows, x-chunks of len.
 void add_stencil_units(std::vector<StencilUnit>& out, int cellidx, const CellDesc& cd, int NT,
-                       int& slot, int chunk_req = 0) {
+                       int& slot, int chunk_req = 0, int variant = 2) {
   const int R = NT / cd.nz;
-  const int maxrows = std::max(1, std::min(R - 1, cd.ny));
+  const int maxrows = std::max(1, std::min(variant == 2 ? 2 * R - 1 : R - 1, cd.ny));
   const int ntiles = (cd.ny + maxrows - 1) / maxrows;
   const int chunk = chunk_req > 0 ? std::min(chunk_req, cd.nx)
                                   : (cd.nx >= 128 ? 32 : (cd.nx >= 64 ? 16 : (cd.nx >= 16 ? 8 : cd.nx)));
@@ -420,8 +430,19 @@ template <typename T> size_t esize() { return sizeof(T); }
 namespace {
 
 template <typename T, int NT, int OUT, int NZ, typename TIn, typename TOut, typename TB, typename TC>
-void stencil_go(femh_handle* H, dim3 grid, size_t smem, const StencilArgs<TIn, TOut, TB, TC>& a) {
-  static bool attr = false;
+void stencil_go(femh_handle* H, dim3 grid, size_t smem, const StencilArgs<TIn, TOut, TB, TC>& a, int variant) {
+  static bool attr1 = false, attr2 = false;
+  if (variant == 2) {
+    auto fn2 = stencil2_kernel<T, NT, OUT, NZ, TIn, TOut, TB, TC>;
+    if (!attr2) {
+      CK(cudaFuncSetAttribute(fn2, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+      attr2 = true;
+    }
+    fn2<<<grid, NT, smem, H->stream>>>(a);
+    LAUNCH_CHECK(H);
+    return;
+  }
+  bool& attr = attr1;
   auto fn = stencil_kernel<T, NT, OUT, NZ, TIn, TOut, TB, TC>;
   if (!attr) {
     CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -435,11 +456,14 @@ void stencil_go(femh_handle* H, dim3 grid, size_t smem, const StencilArgs<TIn, T
 template <typename T, int OUT, typename TIn, typename TOut, typename TB, typename TC>
 void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* out, const TB* b,
              const TC* kc, double* part, const CGState* stt, double omega) {
+  const bool use64 = sizeof(T) == 8 && L.use64 && !smooth_only;
   UnitList& ul = smooth_only ? L.smooth : L.all;
-  if (ul.su.empty()) return;
+  const std::vector<StencilUnit>& units = use64 ? L.su64 : ul.su;
+  if (units.empty()) return;
+  const int variant = use64 ? L.variant64 : L.variant;
   StencilArgs<TIn, TOut, TB, TC> a;
   a.cells = L.d_cells;
-  a.units = ul.d_su;
+  a.units = use64 ? L.d_su64 : ul.d_su;
   a.u = in;
   a.out = out;
   a.b = b;
@@ -450,8 +474,10 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   a.ntot = L.ntot;
   a.k = H->hk;
   a.omega = omega;
-  const size_t smem = 2 * sizeof(T) * (size_t)(15 * L.NT + 3 * L.maxnz) + 16 + 64 * sizeof(double);
-  dim3 grid((unsigned)ul.su.size(), kNumRhs);
+  const size_t smem = variant == 2
+                          ? sizeof(T) * (size_t)(2 * (6 * L.NT + 3 * L.maxnz) + 24 * L.NT) + 16 + 64 * sizeof(double)
+                          : 2 * sizeof(T) * (size_t)(15 * L.NT + 3 * L.maxnz) + 16 + 64 * sizeof(double);
+  dim3 grid((unsigned)units.size(), kNumRhs);
   static const char* mode_names[] = {"apply", "apply_dot", "jacobi", "jacobi_dot", "resid"};
   char nm[64];
   snprintf(nm, sizeof nm, "stencil_%s_%s_L%d", sizeof(T) == 8 ? "f64" : "f32", mode_names[OUT], L.level);
@@ -473,19 +499,19 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   std::string key(nm);
   Prof prof_(H, H->prof ? H->kstats.emplace(key, femh_handle::KStat{}).first->first.c_str() : nm, nodes * per);
   switch (L.nz_spec) {   // compile-time z extent (threads fixed per extent)
-    case 16: stencil_go<T, 512, OUT, 16>(H, grid, smem, a); return;
-    case 24: stencil_go<T, 480, OUT, 24>(H, grid, smem, a); return;
-    case 32: stencil_go<T, 512, OUT, 32>(H, grid, smem, a); return;
-    case 48: stencil_go<T, 480, OUT, 48>(H, grid, smem, a); return;
-    case 64: stencil_go<T, 512, OUT, 64>(H, grid, smem, a); return;
-    case 128: stencil_go<T, 512, OUT, 128>(H, grid, smem, a); return;
-    case 256: stencil_go<T, 512, OUT, 256>(H, grid, smem, a); return;
+    case 16: stencil_go<T, 512, OUT, 16>(H, grid, smem, a, variant); return;
+    case 24: stencil_go<T, 480, OUT, 24>(H, grid, smem, a, variant); return;
+    case 32: stencil_go<T, 512, OUT, 32>(H, grid, smem, a, variant); return;
+    case 48: stencil_go<T, 480, OUT, 48>(H, grid, smem, a, variant); return;
+    case 64: stencil_go<T, 512, OUT, 64>(H, grid, smem, a, variant); return;
+    case 128: stencil_go<T, 512, OUT, 128>(H, grid, smem, a, variant); return;
+    case 256: stencil_go<T, 512, OUT, 256>(H, grid, smem, a, variant); return;
     default: break;
   }
   switch (L.NT) {
-    case 128: stencil_go<T, 128, OUT, 0>(H, grid, smem, a); break;
-    case 256: stencil_go<T, 256, OUT, 0>(H, grid, smem, a); break;
-    case 512: stencil_go<T, 512, OUT, 0>(H, grid, smem, a); break;
+    case 128: stencil_go<T, 128, OUT, 0>(H, grid, smem, a, variant); break;
+    case 256: stencil_go<T, 256, OUT, 0>(H, grid, smem, a, variant); break;
+    case 512: stencil_go<T, 512, OUT, 0>(H, grid, smem, a, variant); break;
     default: throw FemhError{FEMH_E_ARG, "unsupported stencil block size"};
   }
 }
@@ -502,6 +528,7 @@ namespace {
 
 template <typename T>
 void autotune_levels(femh_handle* H, bool mg);
+void autotune_level0_fp64(femh_handle* H);
 
 void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vector<double>& hs) {
   const femh_config& c = H->cfg;
@@ -597,7 +624,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
     for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
       const CellDesc& cd = L.cells[ci];
       L.su_sb.push_back(ss);
-      add_stencil_units(L.all.su, ci, cd, L.NT, ss);
+      add_stencil_units(L.all.su, ci, cd, L.NT, ss, 0, L.variant);
       L.su_se.push_back(ss);
       L.nu_sb.push_back(sn);
       add_node_units(L.all.nu, ci, (long long)cd.nx * cd.ny * cd.nz, sn);
@@ -665,8 +692,9 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
     if (mg32 || (mixed && !gmg)) autotune_levels<float>(H, gmg);
     else autotune_levels<double>(H, gmg);
   }
+  if (mg32 || mixed) autotune_level0_fp64(H);   // FP64 operator of the mixed modes
   const Level& L0 = H->levels[0];
-  H->d_part_s = ar.arr<double>(L0.all.su.size() * kNumRhs);
+  H->d_part_s = ar.arr<double>(std::max(L0.all.su.size(), L0.su64.size()) * kNumRhs);
   H->d_part_n = ar.arr<double>(L0.all.nu.size() * kNumRhs * 2);
   H->d_part_z = ar.arr<double>(L0.all.nu.size() * kNumRhs);
   H->d_part_e = ar.arr<double>(L0.all.nu.size() * 22);   // 21 pair energies + sum of rho per slot
@@ -690,6 +718,46 @@ bool verbose() {
   return v != 0;
 }
 
+
+// Batch compaction: restrict every level's unit lists to cells that still
+// have an iterating load case (slots keep their numbers, so partial sums and
+// per-cell slot ranges stay valid), or restore the full lists.
+struct FullLists {
+  std::vector<StencilUnit> all_su, smooth_su, su64;
+  std::vector<NodeUnit> all_nu, smooth_nu;
+};
+
+void set_units(femh_handle* H, Level& L, const FullLists& F, const std::vector<char>* keep) {
+  auto filt_s = [&](const std::vector<StencilUnit>& in) {
+    std::vector<StencilUnit> out;
+    for (const auto& u : in)
+      if (!keep || (*keep)[L.cells[u.cell].id]) out.push_back(u);
+    return out;
+  };
+  auto filt_n = [&](const std::vector<NodeUnit>& in) {
+    std::vector<NodeUnit> out;
+    for (const auto& u : in)
+      if (!keep || (*keep)[L.cells[u.cell].id]) out.push_back(u);
+    return out;
+  };
+  cudaStream_t s = H->stream;
+  // copies come from the level's own (persistent) host vectors
+  auto put_s = [&](std::vector<StencilUnit>& dst, StencilUnit* d, std::vector<StencilUnit> v) {
+    dst.swap(v);
+    if (!dst.empty())
+      CK(cudaMemcpyAsync(d, dst.data(), sizeof(StencilUnit) * dst.size(), cudaMemcpyHostToDevice, s));
+  };
+  auto put_n = [&](std::vector<NodeUnit>& dst, NodeUnit* d, std::vector<NodeUnit> v) {
+    dst.swap(v);
+    if (!dst.empty()) CK(cudaMemcpyAsync(d, dst.data(), sizeof(NodeUnit) * dst.size(), cudaMemcpyHostToDevice, s));
+  };
+  put_s(L.all.su, L.all.d_su, filt_s(F.all_su));
+  put_s(L.smooth.su, L.smooth.d_su, filt_s(F.smooth_su));
+  if (L.use64) put_s(L.su64, L.d_su64, filt_s(F.su64));
+  put_n(L.all.nu, L.all.d_nu, filt_n(F.all_nu));
+  put_n(L.smooth.nu, L.smooth.d_nu, filt_n(F.smooth_nu));
+}
+
 // (Re)build a level's stencil unit lists for an x-chunk length.
 void build_stencil_units(femh_handle* H, Level& L, int chunk) {
   L.chunk = chunk;
@@ -700,7 +768,7 @@ void build_stencil_units(femh_handle* H, Level& L, int chunk) {
   int ss = 0;
   for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
     L.su_sb.push_back(ss);
-    add_stencil_units(L.all.su, ci, L.cells[ci], L.NT, ss, chunk);
+    add_stencil_units(L.all.su, ci, L.cells[ci], L.NT, ss, chunk, L.variant);
     L.su_se.push_back(ss);
   }
   for (auto& u : L.all.su)
@@ -711,6 +779,80 @@ void build_stencil_units(femh_handle* H, Level& L, int chunk) {
   L.smooth.d_su = upload(ar, L.smooth.su, s);
   L.d_su_sb = upload(ar, L.su_sb, s);
   L.d_su_se = upload(ar, L.su_se, s);
+}
+
+void build_stencil_units64(femh_handle* H, Level& L, int chunk, int variant) {
+  L.use64 = true;
+  L.variant64 = variant;
+  L.chunk64 = chunk;
+  L.su64.clear();
+  L.su64_sb.clear();
+  L.su64_se.clear();
+  int ss = 0;
+  for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
+    L.su64_sb.push_back(ss);
+    add_stencil_units(L.su64, ci, L.cells[ci], L.NT, ss, chunk, variant);
+    L.su64_se.push_back(ss);
+  }
+  cudaStream_t s = H->stream;
+  Arena& ar = H->setup;
+  L.d_su64 = upload(ar, L.su64, s);
+  L.d_su64_sb = upload(ar, L.su64_sb, s);
+  L.d_su64_se = upload(ar, L.su64_se, s);
+}
+
+// FP64 layout of level 0 (mixed modes): variant x chunk timed with the FP64 operator.
+void autotune_level0_fp64(femh_handle* H) {
+  Level& L = H->levels[0];
+  cudaStream_t s = H->stream;
+  std::string key = "f64L0:" + std::to_string(L.NT);
+  int maxnx = 1;
+  for (auto& cd : L.cells) {
+    key += ":" + std::to_string(cd.nx) + "x" + std::to_string(cd.ny) + "x" + std::to_string(cd.nz);
+    maxnx = std::max(maxnx, cd.nx);
+  }
+  auto it = H->tune_cache.find(key);
+  if (it != H->tune_cache.end()) {
+    build_stencil_units64(H, L, it->second / 4, it->second % 4);
+    return;
+  }
+  if (!H->cfg.autotune || L.ntot < 4096) {
+    build_stencil_units64(H, L, 0, 1);
+    H->tune_cache[key] = 0 * 4 + 1;
+    return;
+  }
+  double* in = H->x64;
+  double* out = H->b64;
+  CK(cudaMemsetAsync(H->kc64, 0, sizeof(double) * L.ntot, s));
+  CK(cudaMemsetAsync(in, 0, sizeof(double) * 18 * L.ntot, s));
+  int best = 0, best_var = 1;
+  float best_ms = 1e30f;
+  std::vector<int> cands;
+  for (int cand : {4, 8, 16, 32, 64, maxnx})
+    if (cand <= maxnx && std::find(cands.begin(), cands.end(), cand) == cands.end()) cands.push_back(cand);
+  for (int var : {1, 2})
+    for (int cand : cands) {
+      build_stencil_units64(H, L, cand, var);
+      float ms_min = 1e30f;
+      for (int rep = 0; rep < 3; ++rep) {
+        CK(cudaEventRecord(H->ev0, s));
+        stencil<double, OUT_APPLY>(H, L, false, (const double*)in, out, (const double*)nullptr,
+                                   (const double*)H->kc64, nullptr, nullptr, 0.0);
+        CK(cudaEventRecord(H->ev1, s));
+        CK(cudaEventSynchronize(H->ev1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, H->ev0, H->ev1));
+        ms_min = std::min(ms_min, ms);
+      }
+      if (verbose()) std::fprintf(stderr, "[femh] tune level 0 fp64 variant %d chunk %d: %.4f ms\n", var, cand, ms_min);
+      if (ms_min < best_ms) {
+        best_ms = ms_min;
+        best = cand;
+        best_var = var;
+      }
+    }
+  build_stencil_units64(H, L, best, best_var);
+  H->tune_cache[key] = best * 4 + best_var;
 }
 
 // Project autotuner for the stencil's tile shape: for every level whose
@@ -731,12 +873,13 @@ void autotune_levels(femh_handle* H, bool mg) {
       maxnx = std::max(maxnx, cd.nx);
     }
     auto it = H->tune_cache.find(key);
-    if (it != H->tune_cache.end()) {
-      if (it->second != L.chunk) build_stencil_units(H, L, it->second);
+    if (it != H->tune_cache.end()) {   // cached: chunk * 4 + variant
+      L.variant = it->second % 4;
+      build_stencil_units(H, L, it->second / 4);
       continue;
     }
     if (L.ntot < 4096) {   // tiny levels: launch-bound, the heuristic is fine
-      H->tune_cache[key] = L.chunk;
+      H->tune_cache[key] = L.chunk * 4 + L.variant;
       continue;
     }
     T* in = (T*)(L.xa ? L.xa : H->cg_r);
@@ -744,12 +887,14 @@ void autotune_levels(femh_handle* H, bool mg) {
     CK(cudaMemsetAsync(L.kc, 0, sizeof(T) * L.ntot, s));
     CK(cudaMemsetAsync(L.invd, 0, sizeof(float) * L.ntot, s));
     CK(cudaMemsetAsync(in, 0, sizeof(T) * 18 * L.ntot, s));
-    int best = L.chunk;
+    int best = L.chunk, best_var = L.variant;
     float best_ms = 1e30f;
     std::vector<int> cands;
     for (int cand : {4, 8, 16, 32, 64, maxnx})
       if (cand <= maxnx && std::find(cands.begin(), cands.end(), cand) == cands.end()) cands.push_back(cand);
+    for (int var : {1, 2})
     for (int cand : cands) {
+      L.variant = var;
       build_stencil_units(H, L, cand);
       float ms_min = 1e30f;
       for (int rep = 0; rep < 3; ++rep) {
@@ -762,14 +907,16 @@ void autotune_levels(femh_handle* H, bool mg) {
         CK(cudaEventElapsedTime(&ms, H->ev0, H->ev1));
         ms_min = std::min(ms_min, ms);
       }
-      if (verbose()) std::fprintf(stderr, "[femh] tune level %zu chunk %d: %.4f ms\n", l, cand, ms_min);
+      if (verbose()) std::fprintf(stderr, "[femh] tune level %zu variant %d chunk %d: %.4f ms\n", l, var, cand, ms_min);
       if (ms_min < best_ms) {
         best_ms = ms_min;
         best = cand;
+        best_var = var;
       }
     }
+    L.variant = best_var;
     build_stencil_units(H, L, best);
-    H->tune_cache[key] = best;
+    H->tune_cache[key] = best * 4 + best_var;
   }
 }
 
@@ -948,7 +1095,9 @@ void pcg_iteration(femh_handle* H, const typename PR::K* kcg) {
   stencil<TV, OUT_APPLY_DOT>(H, L0, false, (const TP*)p, q, (const TV*)nullptr, kcg, H->d_part_s, stt, 0.0);
   {
     Prof prof_(H, "k_fin_alpha", 0.0);
-    k_fin_alpha<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_su_sb, L0.d_su_se, H->d_part_s, nc);
+    const bool l64 = sizeof(TV) == 8 && L0.use64;   // the apply above used the FP64 layout
+    k_fin_alpha<<<fin_blocks(nc), 128, 0, s>>>(stt, l64 ? L0.d_su64_sb : L0.d_su_sb,
+                                               l64 ? L0.d_su64_se : L0.d_su_se, H->d_part_s, nc);
     LAUNCH_CHECK(H);
   }
   {
@@ -1021,25 +1170,27 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
     }
     TM* z = vcycle<TM, TMC, TV>(H, r);
     {
-      Prof prof_(H, "k_copy", 0.0);
-      k_copy<TP, TM><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, p, z, stt, L0.ntot);
-      LAUNCH_CHECK(H);
-    }
-    {
       Prof prof_(H, "k_dot", 0.0);
       k_dot<TM, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
       LAUNCH_CHECK(H);
     }
     {
       Prof prof_(H, "k_fin_rz", 0.0);
-      k_fin_rz<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_z, nc);
+      k_fin_rz<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_z, H->d_part_n, nc);
+      LAUNCH_CHECK(H);
+    }
+    {   // p = z (beta = 0; Jacobi z for pairs that fell back)
+      Prof prof_(H, "k_cg_dir", 0.0);
+      k_cg_dir<TP, TM, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, p, (const TM*)z,
+                                                             (const TV*)r, L0.invd, stt, L0.ntot);
       LAUNCH_CHECK(H);
     }
   }
   const int chunk = H->prof ? 1 : std::max(1, c.graph_chunk > 0 ? c.graph_chunk : 8);
   cudaGraphExec_t exec = nullptr;
   long long graph_kernels = 0;
-  if (c.graph_chunk > 0 && !H->prof) {
+  auto capture = [&]() {
+    if (!(c.graph_chunk > 0 && !H->prof)) return;
     cudaGraph_t g = nullptr;
     H->capturing = true;
     H->cap_count = 0;
@@ -1057,7 +1208,16 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
     CK(cudaStreamEndCapture(s, &g));
     CK(cudaGraphInstantiate(&exec, g, 0));
     cudaGraphDestroy(g);
-  }
+  };
+  // batch compaction bookkeeping
+  std::vector<FullLists> full;
+  int listed = nc;   // cells covered by the current unit lists
+  auto restore = [&]() {
+    if (full.empty()) return;
+    for (size_t l = 0; l < H->levels.size(); ++l) set_units(H, H->levels[l], full[l], nullptr);
+    full.clear();
+  };
+  capture();
   int done = 0;
   try {
     while (true) {
@@ -1071,15 +1231,36 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
       CK(cudaMemcpyAsync(H->state.data(), stt, sizeof(CGState) * H->state.size(), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
       prof_resolve(H);
-      bool any = false;
-      for (auto& S : H->state) any |= (S.active != 0);
-      if (!any || done > max_iter + chunk) break;
+      std::vector<char> keep(nc, 0);
+      int alive = 0;
+      for (int t = 0; t < nc * kNumRhs; ++t)
+        if (H->state[t].active) keep[t / kNumRhs] = 1;
+      for (int ci = 0; ci < nc; ++ci) alive += keep[ci];
+      if (alive == 0 || done > max_iter + chunk) break;
+      if (nc > 1 && 2 * alive <= listed) {   // at least half of the listed cells finished: compact
+        if (full.empty()) {
+          full.resize(H->levels.size());
+          for (size_t l = 0; l < H->levels.size(); ++l) {
+            Level& L = H->levels[l];
+            full[l] = FullLists{L.all.su, L.smooth.su, L.su64, L.all.nu, L.smooth.nu};
+          }
+        }
+        for (size_t l = 0; l < H->levels.size(); ++l) set_units(H, H->levels[l], full[l], &keep);
+        listed = alive;
+        if (exec) {
+          CK(cudaGraphExecDestroy(exec));
+          exec = nullptr;
+        }
+        capture();
+      }
     }
   } catch (...) {
     if (exec) cudaGraphExecDestroy(exec);
+    restore();
     throw;
   }
   if (exec) CK(cudaGraphExecDestroy(exec));
+  restore();
   for (int t = 0; t < nc * kNumRhs; ++t) iters_out[t] += H->state[t].iters;
 }
 
@@ -1337,7 +1518,7 @@ femh_status femh_config_default(femh_config* c) {
   c->solver = FEMH_GMG_PCG;
   c->pre_smooth = 2;
   c->post_smooth = 2;
-  c->omega = 0.4;
+  c->omega = 0.35;   // < 2 / 5.36: damped Jacobi stable for any coefficient field (nu = 0.3)
   c->coarse_max_nodes = 64;
   c->tol = 1e-10;
   c->max_iter = 20000;

@@ -65,7 +65,8 @@ struct CGState {
   double rz, pq, alpha, beta, rr, bnorm2, rel, scale;
   int iters, active, status, max_iter;
   double tol;
-  int outer, pad;   // defect correction: this (cell, rhs) takes part in the current outer step
+  int outer;        // defect correction: this (cell, rhs) takes part in the current outer step
+  int fallback;     // 1: the multigrid preconditioner turned indefinite; Jacobi from then on
 };
 enum CGStatus : int { CG_RUNNING = 0, CG_CONVERGED = 1, CG_MAXITER = 2, CG_BREAKDOWN = 3 };
 

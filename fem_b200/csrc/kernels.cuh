@@ -172,11 +172,9 @@ __global__ void k_cg_init(const CellDesc* cells, const NodeUnit* units, const TB
         st_val(x + o, 0.0);
         st_val(r + o, rv);
         v[0] += rv * rv;
-        if (jacobi) {
-          const double z = (double)id * rv;
-          v[1] += rv * z;
-          st_val(p + o, z);
-        }
+        const double z = (double)id * rv;
+        v[1] += rv * z;
+        if (jacobi) st_val(p + o, z);
       }
     }
   }
@@ -244,8 +242,8 @@ __global__ void k_cg_dir(const CellDesc* cells, const NodeUnit* units, TP* __res
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long o = ((long long)rhs * 3 + c) * ntot + g;
-      const double z = zvec ? (double)ld_val(zvec + o) : (double)invd[g] * (double)ld_val(r + o);
-      st_val(p + o, z + be * (double)ld_val(p + o));
+      const double z = (zvec && !S.fallback) ? (double)ld_val(zvec + o) : (double)invd[g] * (double)ld_val(r + o);
+      st_val(p + o, be == 0.0 ? z : z + be * (double)ld_val(p + o));
     }
   }
 }
@@ -288,13 +286,23 @@ __global__ void k_fin_init(CGState* stt, const int* slot_begin, const int* slot_
   if (lead) stt[t] = S;
 }
 
-// rz for the multigrid preconditioner at start (z0 . r from the V-cycle's last sweep).
+// rz for the multigrid preconditioner at start (z . r of the first V-cycle);
+// if that is not positive, the pair starts with the Jacobi preconditioner.
+// beta = 0 so that the following direction kernel sets p = z.
 __global__ void k_fin_rz(CGState* stt, const int* slot_begin, const int* slot_end,
-                         const double* part, int ncells) {
+                         const double* part, const double* part_init, int ncells) {
   FIN_PROLOGUE
   CGState S = stt[t];
   if (!S.active) return;
-  S.rz = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 1, 0);
+  const double rz_mg = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 1, 0);
+  const double rz_jac = sum_slots(part_init, slot_begin[cell], slot_end[cell], rhs, 2, 1);
+  S.beta = 0.0;
+  if (isfinite(rz_mg) && rz_mg > 0.0) {
+    S.rz = rz_mg;
+  } else {
+    S.fallback = 1;
+    S.rz = rz_jac;
+  }
   if (lead) stt[t] = S;
 }
 
@@ -325,7 +333,9 @@ __global__ void k_fin_beta(CGState* stt, const int* slot_begin, const int* slot_
   if (!S.active) return;
   const int b = slot_begin[cell], e = slot_end[cell];
   const double rr = sum_slots(part_upd, b, e, rhs, 2, 0);
-  const double rzn = jacobi ? sum_slots(part_upd, b, e, rhs, 2, 1) : sum_slots(part_rz, b, e, rhs, 1, 0);
+  const double rz_jac = sum_slots(part_upd, b, e, rhs, 2, 1);
+  const double rz_mg = jacobi ? rz_jac : sum_slots(part_rz, b, e, rhs, 1, 0);
+  const double rzn = (jacobi || S.fallback) ? rz_jac : rz_mg;
   S.rr = rr;
   S.iters += 1;
   S.rel = sqrt(rr / S.bnorm2);
@@ -336,8 +346,16 @@ __global__ void k_fin_beta(CGState* stt, const int* slot_begin, const int* slot_
     S.active = 0;
     S.status = CG_MAXITER;
   } else if (!isfinite(rzn) || !(rzn > 0.0)) {
-    S.active = 0;
-    S.status = CG_BREAKDOWN;
+    if (!jacobi && !S.fallback && isfinite(rz_jac) && rz_jac > 0.0) {
+      // the V-cycle is not positive definite for this field: restart the
+      // search direction with the (always SPD) Jacobi preconditioner
+      S.fallback = 1;
+      S.beta = 0.0;
+      S.rz = rz_jac;
+    } else {
+      S.active = 0;
+      S.status = CG_BREAKDOWN;
+    }
   } else {
     S.beta = rzn / S.rz;
     S.rz = rzn;

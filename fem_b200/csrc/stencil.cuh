@@ -327,3 +327,259 @@ inline size_t stencil_smem_bytes(int NT, int nz) {
 }
 
 }  // namespace femh
+
+namespace femh {
+
+// Two voxel rows per thread.  Thread (t, z) of a CTA streams voxels
+// (i, e0, z) and (i, e0+1, z), e0 = j0-1+2t, along x.  Node rows n0 = e0,
+// n1 = e0+1, n2 = e0+2: the y coupling of its two voxels (node row n1) stays in
+// registers; it owns node rows n1 and n2 (n2 needs the lower-y corners of the
+// next thread row's first voxel).  Owned rows per tile: 2*TR-1 for TR thread
+// rows.  Shared memory per step: node plane P (slots 2t, 2t+1, 2t+2 hold rows
+// n0, n1, n2 of thread t; slot 0 is the halo row loaded by t = 0) and corner
+// totals Q (A: node (n1, z+1); B: (n2, z+1); C: (n0, z); D: (n0, z+1)), both
+// double-buffered, one barrier per step.
+template <typename T, int NT, int OUT, int NZ, typename TIn, typename TOut, typename TB, typename TC>
+__global__ void __launch_bounds__(NT, 1)
+stencil2_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const StencilUnit un = a.units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cd = a.cells[un.cell];
+  if (a.stt && !a.stt[cd.id * kNumRhs + rhs].active) return;
+  const int nx = cd.nx, ny = cd.ny;
+  const int nz = NZ > 0 ? NZ : cd.nz;
+  const int TR = NT / nz;
+  const int tid = threadIdx.x;
+  const int t = tid / nz, z = tid - t * nz;
+  const int rows = un.rows;
+  const bool live = t < TR && 2 * t <= rows;
+  const bool own1 = live && 2 * t < rows;
+  const bool own2 = live && 2 * t + 1 < rows;
+  const int zp = (z + 1 == nz) ? 0 : z + 1;
+  const int zm = (z == 0) ? nz - 1 : z - 1;
+  auto wrapy = [&](int j) { j %= ny; return j < 0 ? j + ny : j; };
+  const int n0 = wrapy(un.j0 - 1 + 2 * t), n1 = wrapy(n0 + 1), n2 = wrapy(n0 + 2);
+
+  const size_t PS = (size_t)(2 * TR + 1) * 3 * nz;
+  const size_t QS = (size_t)TR * 12 * nz;
+  T* P = reinterpret_cast<T*>(smem_raw);   // [2][2TR+1][3][nz]
+  T* Q = P + 2 * PS;                       // [2][TR][4][3][nz]
+  double* red = reinterpret_cast<double*>(smem_raw + ((sizeof(T) * (2 * PS + 2 * QS) + 15) & ~(size_t)15));
+  const size_t s0 = (size_t)(2 * t) * 3 * nz;   // slot of row n0; n1 at +3nz, n2 at +6nz
+  const size_t qt = (size_t)t * 12 * nz;
+  const size_t qn = (size_t)(t + 1 < TR ? t + 1 : t) * 12 * nz;
+
+  const long long st = a.ntot;
+  const long long plane = (long long)ny * nz;
+  const long long cellsz = (long long)nx * plane;
+  const TIn* ub = a.u + (long long)rhs * 3 * st + cd.off;
+  const long long c0 = (long long)n0 * nz + z, c1 = (long long)n1 * nz + z, c2 = (long long)n2 * nz + z;
+  const TC* kcb = a.kc + cd.off;
+  const TB* bb = (OUT >= OUT_JACOBI) ? a.b + (long long)rhs * 3 * st + cd.off : nullptr;
+  const float* ib = a.invd + cd.off;
+  TOut* obase = a.out + (long long)rhs * 3 * st + cd.off;
+
+  T l0[3] = {0, 0, 0}, l1[3] = {0, 0, 0}, l2[3] = {0, 0, 0};   // next node plane, rows n0(t=0 only), n1, n2
+  T k0v = 0, k1v = 0, k0n = 0, k1n = 0;                        // kc of voxel rows e0, e1
+  T prev[3][2][3];          // [row n0..n2][z, z+1][comp], node plane ie
+  T carry[3][2][3];         // upper-x contributions of the voxel pair, by node position
+  T own1v[3] = {0, 0, 0}, own2v[3] = {0, 0, 0}, u1[3] = {0, 0, 0}, u2[3] = {0, 0, 0};
+  T eb1[3] = {0, 0, 0}, eb2[3] = {0, 0, 0};
+  T id1 = 0, id2 = 0;
+  long long pg = 0;
+  double acc = 0.0;
+
+  auto adv = [&](long long& o) { o += plane; if (o >= cellsz) o -= cellsz; };
+  auto load_plane = [&](long long po) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (t == 0) l0[c] = (T)ld_val(ub + c * st + po + c0);
+      l1[c] = (T)ld_val(ub + c * st + po + c1);
+      l2[c] = (T)ld_val(ub + c * st + po + c2);
+    }
+  };
+  auto store_plane = [&](T* Pb) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (t == 0) Pb[s0 + c * nz + z] = l0[c];
+      Pb[s0 + (3 + c) * nz + z] = l1[c];
+      Pb[s0 + (6 + c) * nz + z] = l2[c];
+    }
+  };
+  auto epilogue = [&](T (&y)[3], const T (&un_)[3], const T (&ebv)[3], T idv, long long node) {
+    TOut* ob = obase + node;
+    if (OUT == OUT_APPLY || OUT == OUT_APPLY_DOT) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        st_val(ob + c * st, y[c]);
+        if (OUT == OUT_APPLY_DOT) acc += (double)un_[c] * (double)y[c];
+      }
+    } else {
+      const bool pin = (node == 0);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (OUT == OUT_RESID) {
+          st_val(ob + c * st, pin ? (T)0 : ebv[c] - y[c]);
+        } else {
+          const T xv = un_[c] + (T)a.omega * idv * (ebv[c] - y[c]);
+          st_val(ob + c * st, xv);
+          if (OUT == OUT_JACOBI_DOT) acc += (double)xv * (double)ebv[c];
+        }
+      }
+    }
+  };
+  auto gather = [&](const T* Qg) {
+    if (own1) {
+      T y[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) y[c] = own1v[c] + Qg[qt + (0 * 3 + c) * nz + zm];
+      epilogue(y, u1, eb1, id1, pg + c1);
+    }
+    if (own2) {
+      T y[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        y[c] = own2v[c] + Qg[qt + (1 * 3 + c) * nz + zm] + Qg[qn + (2 * 3 + c) * nz + z] +
+               Qg[qn + (3 * 3 + c) * nz + zm];
+      epilogue(y, u2, eb2, id2, pg + c2);
+    }
+  };
+
+  // prologue: node plane i0-1 -> prev (via P[1])
+  long long pk = (long long)((un.i0 - 1 + nx) % nx) * plane;
+  long long pn = pk;
+  if (live) {
+    load_plane(pn);
+    k0n = (T)ld_val(kcb + pk + c0);
+    k1n = (T)ld_val(kcb + pk + c1);
+    store_plane(P + PS);
+  }
+  __syncthreads();
+  adv(pn);
+  if (live) {
+    const T* Pr = P + PS + s0;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        prev[r][0][c] = Pr[(3 * r + c) * nz + z];
+        prev[r][1][c] = Pr[(3 * r + c) * nz + zp];
+        carry[r][0][c] = carry[r][1][c] = (T)0;
+      }
+    load_plane(pn);
+  }
+
+  for (int s = 0; s <= un.len; ++s) {
+    const long long pe = pk;   // voxel plane ie = i0-1+s
+    T* Pb = P + (s & 1) * PS;
+    T* Qb = Q + (s & 1) * QS;
+    if (live) {
+      store_plane(Pb);
+      k0v = k0n;
+      k1v = k1n;
+      if (s < un.len) {
+        adv(pn);
+        adv(pk);
+        load_plane(pn);
+        k0n = (T)ld_val(kcb + pk + c0);
+        k1n = (T)ld_val(kcb + pk + c1);
+      }
+    }
+    __syncthreads();
+    if (s >= 2) gather(Q + ((s - 1) & 1) * QS);
+    if (OUT >= OUT_JACOBI && s >= 1) {
+      if (own1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) eb1[c] = (T)ld_val(bb + c * st + pe + c1);
+        if (OUT != OUT_RESID) id1 = (T)ib[pe + c1];
+      }
+      if (own2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) eb2[c] = (T)ld_val(bb + c * st + pe + c2);
+        if (OUT != OUT_RESID) id2 = (T)ib[pe + c2];
+      }
+    }
+    if (live) {
+      T cur[3][2][3];
+      const T* Pr = Pb + s0;
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          cur[r][0][c] = Pr[(3 * r + c) * nz + z];
+          cur[r][1][c] = Pr[(3 * r + c) * nz + zp];
+        }
+      T tot[3][2][3], nc[3][2][3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            tot[r][q][c] = carry[r][q][c];
+            nc[r][q][c] = (T)0;
+          }
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {   // voxel rows e0 (node rows 0,1) and e1 (rows 1,2)
+        T w[3][8];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+#pragma unroll
+          for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+            for (int az = 0; az < 2; ++az) {
+              w[c][2 * ay + az] = prev[e + ay][az][c];
+              w[c][4 + 2 * ay + az] = cur[e + ay][az][c];
+            }
+          fwht8_fwd(w[c]);
+        }
+        had_block(w, a.k, e == 0 ? k0v : k1v);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          fwht8_inv(w[c]);
+#pragma unroll
+          for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+            for (int az = 0; az < 2; ++az) {
+              tot[e + ay][az][c] += w[c][2 * ay + az];
+              nc[e + ay][az][c] += w[c][4 + 2 * ay + az];
+            }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        u1[c] = prev[1][0][c];
+        u2[c] = prev[2][0][c];
+        own1v[c] = tot[1][0][c];
+        own2v[c] = tot[2][0][c];
+        if (s > 0) {
+          Qb[qt + (0 * 3 + c) * nz + z] = tot[1][1][c];   // A: node (n1, z+1)
+          Qb[qt + (1 * 3 + c) * nz + z] = tot[2][1][c];   // B: node (n2, z+1)
+          Qb[qt + (2 * 3 + c) * nz + z] = tot[0][0][c];   // C: node (n0, z)
+          Qb[qt + (3 * 3 + c) * nz + z] = tot[0][1][c];   // D: node (n0, z+1)
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            carry[r][q][c] = nc[r][q][c];
+            prev[r][q][c] = cur[r][q][c];
+          }
+      pg = pe;
+    }
+  }
+  __syncthreads();
+  if (un.len >= 1) gather(Q + (un.len & 1) * QS);
+
+  if (OUT == OUT_APPLY_DOT || OUT == OUT_JACOBI_DOT) {
+    double v[1] = {acc};
+    block_reduce<1>(v, red);
+    if (tid == 0) a.partials[(long long)un.slot * kNumRhs + rhs] = v[0];
+  }
+}
+
+}  // namespace femh

@@ -125,7 +125,7 @@ class Config:
     solver: int = GMG_PCG
     pre_smooth: int = 2
     post_smooth: int = 2
-    omega: float = 0.4
+    omega: float = 0.35
     coarse_max_nodes: int = 64
     tol: float = 1e-10
     max_iter: int = 20000
@@ -217,6 +217,7 @@ class Engine:
         """C^H (6x6 numpy) and the solve info of one periodic cell.
 
         rho: (nx, ny, nz) float64 numpy array (host) or CUDA torch tensor."""
+        self._autograd_rho = None
         nx, ny, nz = (int(s) for s in rho.shape)
         if isinstance(rho, np.ndarray):
             rho = np.ascontiguousarray(rho, dtype=np.float64)

@@ -110,6 +110,48 @@ std::vector<double> FEM3DFun::df() {
   return grad;
 }
 
+// ------------------------------------------------------------ descent loop
+void clampVector(std::vector<double>& x, const std::vector<double>& lo, const std::vector<double>& hi) {
+  for (size_t i = 0; i < x.size(); ++i) {
+    if (i < lo.size()) x[i] = std::max(x[i], lo[i]);
+    if (i < hi.size()) x[i] = std::min(x[i], hi[i]);
+  }
+}
+
+int lineSearch(RealFun* fun, std::vector<double>& x0, const std::vector<double>& dir, double& h) {
+  const double f0 = fun->f();
+  for (int step = 0; step < 10; ++step) {
+    std::vector<double> x(x0.size());
+    for (size_t i = 0; i < x.size(); ++i) x[i] = x0[i] - h * dir[i];
+    clampVector(x, fun->lowerBounds, fun->upperBounds);
+    fun->setParam(x);
+    if (fun->f() < f0) {
+      x0 = x;
+      return 0;
+    }
+    h /= 2;
+  }
+  fun->setParam(x0);   // leave the objective at the last accepted point
+  return -1;
+}
+
+int gradientDescent(RealFun* fun, std::vector<double>& x0, int nSteps, double maxStep) {
+  std::vector<double> x = x0;
+  fun->setParam(x);
+  int accepted = 0;
+  for (int it = 0; it < nSteps; ++it) {
+    const std::vector<double> grad = fun->df();
+    double norm = 0.0;
+    for (double g : grad) norm = std::max(norm, std::fabs(g));
+    if (!(norm > 0.0)) break;
+    double h = maxStep / norm;
+    if (lineSearch(fun, x, grad, h) < 0) break;
+    x0 = x;
+    ++accepted;
+  }
+  return accepted;
+}
+
 // ----------------------------------------------- NumericalCoarseningUsingMultigrid
 void fromLamesParametersToYoungModulusPoissonRatio(double lambda, double mu, double& E, double& nu) {
   E = mu * (3 * lambda + 2 * mu) / (lambda + mu);

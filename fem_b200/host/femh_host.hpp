@@ -96,6 +96,15 @@ class FEM3DFun : public RealFun {
   void ensure_handle();
 };
 
+// Optimisation loop around the objective (fast_fem/run3d.cpp:238-289): steepest
+// descent with a halving line search on the bounds-clamped step x - h*grad.
+void clampVector(std::vector<double>& x, const std::vector<double>& lo, const std::vector<double>& hi);
+// Returns 0 and updates x0 when f decreased within 10 halvings of h, else -1.
+int lineSearch(RealFun* fun, std::vector<double>& x0, const std::vector<double>& dir, double& h);
+// nSteps of descent from x0 with initial step maxStep / ||grad||_inf; x0 holds
+// the last accepted point.  Returns the number of accepted steps.
+int gradientDescent(RealFun* fun, std::vector<double>& x0, int nSteps, double maxStep);
+
 // --------------------------------------------------------- SamplesGenerator ---
 struct BaseMaterial {   // StrainLin parameters: param[0] = mu, param[1] = lambda
   double mu, lambda;

@@ -66,6 +66,15 @@ int main() {
     an.push_back(g[k]);
   }
   fun.setParam(x0);
+  // a few descent steps (fast_fem/run3d.cpp:268-289): f must decrease
+  std::vector<double> xo = x0;
+  fun.lowerBounds.assign(x0.size(), 1e-3);
+  fun.upperBounds.assign(x0.size(), 1.0);
+  const int accepted = gradientDescent(&fun, xo, 3, 0.05);
+  const double f_after = fun.f();
+  if (accepted < 1 || !(f_after < f0)) ++fails;
+  std::printf("\"descent_f\": [%.17g, %.17g], \"descent_steps\": %d,\n", f0, f_after, accepted);
+  fun.setParam(x0);
   std::printf("\"f\": %.17g,\n", f0);
   std::printf("\"density\": %.17g,\n", fun.density);
   print_vec("G", G);

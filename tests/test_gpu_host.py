@@ -63,3 +63,10 @@ def test_coarsening_outputs(host_out, oracle):
 
 def test_binary_roundtrip(host_out):
     assert host_out["binary_roundtrip"] and host_out["fails"] == 0
+
+
+def test_gradient_descent_decreases_objective(host_out):
+    """femh_host::gradientDescent (fast_fem/run3d.cpp:268-289 restated) on the
+    FEM3DFun objective: at least one accepted step, f strictly lower."""
+    f0, f1 = host_out["descent_f"]
+    assert host_out["descent_steps"] >= 1 and f1 < f0
