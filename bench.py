@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--impl", default="femh", choices=["femh", "reference"])
     ap.add_argument("--n", type=int, default=N)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="heuristic tile shapes (the first stencil launches are then the solve's own)")
     ap.add_argument("--quick", action="store_true",
                     help="timed device steps only (no e2e / FP64 / roofline / CPU legs): the profiling command")
     return ap.parse_args()
@@ -169,7 +171,7 @@ def main():
     Ct = F.Engine(F.Config(device=local)).homogenize(fields.smooth_cell(n, 4.0, seed=5))[0]
 
     stream = torch.cuda.current_stream()
-    cfg = F.Config(device=local, precision=F.MIXED_PC, solver=F.GMG_PCG)
+    cfg = F.Config(device=local, precision=F.MIXED_PC, solver=F.GMG_PCG, autotune=0 if args.no_autotune else 1)
     eng = F.Engine(cfg)
     eng.set_stream(stream.cuda_stream)
     rho_d = torch.from_numpy(rho_h).cuda()
