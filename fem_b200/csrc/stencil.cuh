@@ -510,77 +510,42 @@ stencil2_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
           cur[r][0][c] = Pr[(3 * r + c) * nz + z];
           cur[r][1][c] = Pr[(3 * r + c) * nz + zp];
         }
-      // Separable Hadamard transform shared by the two voxels: the x and z
-      // butterfly stages are per node row (row 1 serves both voxels), the y
-      // stage per voxel; the inverse runs the y stage per voxel, sums the two
-      // voxels' row-1 parts, then the x and z stages per row.
-      // v[r][c][2kx+kz]: row r after the forward x and z stages.
-      auto row_fwd = [&](int r, T (&v)[3][4]) {
+      T tot[3][2][3], nc[3][2][3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const T sx0 = cur[r][0][c] + prev[r][0][c], dx0 = cur[r][0][c] - prev[r][0][c];
-          const T sx1 = cur[r][1][c] + prev[r][1][c], dx1 = cur[r][1][c] - prev[r][1][c];
-          v[c][0] = sx1 + sx0;
-          v[c][1] = sx1 - sx0;
-          v[c][2] = dx1 + dx0;
-          v[c][3] = dx1 - dx0;
-        }
-      };
-      // one voxel from rows (lo, hi) after the row stages; returns the inverse
-      // y-stage outputs for its lower (ay = 0) and upper (ay = 1) rows
-      auto voxel = [&](const T (&vl)[3][4], const T (&vh)[3][4], T kc, T (&ol)[3][4], T (&oh)[3][4]) {
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            tot[r][q][c] = carry[r][q][c];
+            nc[r][q][c] = (T)0;
+          }
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {   // voxel rows e0 (node rows 0,1) and e1 (rows 1,2)
         T w[3][8];
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
+        for (int c = 0; c < 3; ++c) {
 #pragma unroll
-          for (int kx = 0; kx < 2; ++kx)
+          for (int ay = 0; ay < 2; ++ay)
 #pragma unroll
-            for (int kz = 0; kz < 2; ++kz) {
-              w[c][4 * kx + kz] = vh[c][2 * kx + kz] + vl[c][2 * kx + kz];       // ky = 0
-              w[c][4 * kx + 2 + kz] = vh[c][2 * kx + kz] - vl[c][2 * kx + kz];   // ky = 1
+            for (int az = 0; az < 2; ++az) {
+              w[c][2 * ay + az] = prev[e + ay][az][c];
+              w[c][4 + 2 * ay + az] = cur[e + ay][az][c];
             }
-        had_block(w, a.k, kc);
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-          for (int kx = 0; kx < 2; ++kx)
-#pragma unroll
-            for (int kz = 0; kz < 2; ++kz) {
-              ol[c][2 * kx + kz] = w[c][4 * kx + kz] - w[c][4 * kx + 2 + kz];
-              oh[c][2 * kx + kz] = w[c][4 * kx + kz] + w[c][4 * kx + 2 + kz];
-            }
-      };
-      // inverse x and z stages of one row: lower-x plane -> tot (with the carry),
-      // upper-x plane -> carry
-      auto row_inv = [&](int r, const T (&g)[3][4], T (&totr)[2][3]) {
+          fwht8_fwd(w[c]);
+        }
+        had_block(w, a.k, e == 0 ? k0v : k1v);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const T a00 = g[c][0] - g[c][1], a01 = g[c][0] + g[c][1];   // kx = 0; az = 0, 1
-          const T a10 = g[c][2] - g[c][3], a11 = g[c][2] + g[c][3];   // kx = 1
-          totr[0][c] = carry[r][0][c] + (a00 - a10);
-          totr[1][c] = carry[r][1][c] + (a01 - a11);
-          carry[r][0][c] = a00 + a10;
-          carry[r][1][c] = a01 + a11;
+          fwht8_inv(w[c]);
+#pragma unroll
+          for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+            for (int az = 0; az < 2; ++az) {
+              tot[e + ay][az][c] += w[c][2 * ay + az];
+              nc[e + ay][az][c] += w[c][4 + 2 * ay + az];
+            }
         }
-      };
-      T tot[3][2][3];
-      {
-        T v0[3][4], v1[3][4];
-        row_fwd(0, v0);
-        row_fwd(1, v1);
-        T o0[3][4], o1a[3][4];
-        voxel(v0, v1, k0v, o0, o1a);
-        row_inv(0, o0, tot[0]);
-        T v2[3][4];
-        row_fwd(2, v2);
-        T o1b[3][4], o2[3][4];
-        voxel(v1, v2, k1v, o1b, o2);
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-          for (int q = 0; q < 4; ++q) o1a[c][q] += o1b[c][q];
-        row_inv(1, o1a, tot[1]);
-        row_inv(2, o2, tot[2]);
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -600,7 +565,10 @@ stencil2_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
 #pragma unroll
         for (int q = 0; q < 2; ++q)
 #pragma unroll
-          for (int c = 0; c < 3; ++c) prev[r][q][c] = cur[r][q][c];
+          for (int c = 0; c < 3; ++c) {
+            carry[r][q][c] = nc[r][q][c];
+            prev[r][q][c] = cur[r][q][c];
+          }
       pg = pe;
     }
   }
