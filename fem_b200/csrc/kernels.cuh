@@ -402,35 +402,53 @@ __global__ void k_restrict(const CellDesc* fine, const CellDesc* coarse, const N
 }
 
 // Trilinear prolongation and correction: xf(n) += sum_I w(n,I) ec(I).
+// Each thread corrects the two fine nodes 2m and 2m+1 of a z row, which share
+// the coarse z nodes m and m+1 (fine 2m = coarse m; fine 2m+1 = mean of m, m+1);
+// x and y weights are uniform along the row.  The pinned node 0 keeps 0.
+// (All multigrid levels have even fine extents, so pairs never straddle rows.)
 template <typename TF, typename TCo>
-__global__ void k_prolong_add(const CellDesc* fine, const CellDesc* coarse, const NodeUnit* units,
-                              TF* __restrict__ xf, const TCo* __restrict__ ec, const CGState* stt, long long ntf, long long ntc) {
+__global__ void k_prolong_add(const CellDesc* __restrict__ fine, const CellDesc* __restrict__ coarse,
+                              const NodeUnit* __restrict__ units, TF* __restrict__ xf,
+                              const TCo* __restrict__ ec, const CGState* stt, long long ntf, long long ntc) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cf = fine[u.cell], cc = coarse[fine[u.cell].child];
   if (stt && !stt[cf.id * kNumRhs + rhs].active) return;
-  #pragma unroll 4
-  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+  const long long pb = (u.begin + 1) >> 1, pe = (u.end + 1) >> 1;   // node pairs of the unit
+  for (long long pr = pb + threadIdx.x; pr < pe; pr += blockDim.x) {
+    const long long n = 2 * pr;
     int i, j, k;
-    node_ijk(n, cf.ny, cf.nz, i, j, k);
-    const int ci0 = i >> 1, cj0 = j >> 1, ck0 = k >> 1;
-    const int nxi = (i & 1) ? 2 : 1, nyj = (j & 1) ? 2 : 1, nzk = (k & 1) ? 2 : 1;
-    const double wx = (i & 1) ? 0.5 : 1.0, wy = (j & 1) ? 0.5 : 1.0, wz = (k & 1) ? 0.5 : 1.0;
-    double acc[3] = {0, 0, 0};
-    for (int a = 0; a < nxi; ++a)
-      for (int b = 0; b < nyj; ++b)
-        for (int d = 0; d < nzk; ++d) {
-          const long long g = cc.off + lin(wrap(ci0 + a, cc.nx), wrap(cj0 + b, cc.ny), wrap(ck0 + d, cc.nz),
-                                           cc.ny, cc.nz);
-          const double w = wx * wy * wz;
+    node_ijk(n, cf.ny, cf.nz, i, j, k);   // k even
+    const int ci0 = i >> 1, cj0 = j >> 1, m = k >> 1;
+    const int ci1 = wrap(ci0 + (i & 1), cc.nx), cj1 = wrap(cj0 + (j & 1), cc.ny);
+    const int m1 = wrap(m + 1, cc.nz);
+    const double wx = (i & 1) ? 0.5 : 1.0, wy = (j & 1) ? 0.5 : 1.0;
+    double a0[3] = {0, 0, 0}, a1[3] = {0, 0, 0};   // at fine k = 2m and 2m+1
 #pragma unroll
-          for (int c = 0; c < 3; ++c) acc[c] += w * (double)ld_val(ec + ((long long)rhs * 3 + c) * ntc + g);
+    for (int ax = 0; ax < 2; ++ax) {
+      if (ax == 1 && !(i & 1)) break;
+      const int ci = ax ? ci1 : ci0;
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay) {
+        if (ay == 1 && !(j & 1)) break;
+        const int cj = ay ? cj1 : cj0;
+        const double w = wx * wy;
+        const long long g0 = cc.off + lin(ci, cj, m, cc.ny, cc.nz);
+        const long long g1 = cc.off + lin(ci, cj, m1, cc.ny, cc.nz);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double e0 = (double)ld_val(ec + ((long long)rhs * 3 + c) * ntc + g0);
+          const double e1 = (double)ld_val(ec + ((long long)rhs * 3 + c) * ntc + g1);
+          a0[c] += w * e0;
+          a1[c] += w * 0.5 * (e0 + e1);
         }
-    if (n == 0) continue;   // pinned node keeps 0
+      }
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       TF* px = xf + ((long long)rhs * 3 + c) * ntf + cf.off + n;
-      st_val(px, (double)ld_val(px) + acc[c]);
+      if (n != 0) st_val(px, (double)ld_val(px) + a0[c]);
+      if (n + 1 < u.end) st_val(px + 1, (double)ld_val(px + 1) + a1[c]);
     }
   }
 }
