@@ -285,6 +285,7 @@ struct femh_handle {
   void* cg_r = nullptr;
   void* cg_p = nullptr;
   void* cg_q = nullptr;
+  void* cg_rm = nullptr;        // FP32 copy of the FP64 residual (level-0 rhs of an FP32 V-cycle)
   CGState* d_state = nullptr;
   std::vector<CGState> state;
   double* d_part_s = nullptr;   // stencil partials [slots][6]
@@ -398,7 +399,8 @@ MatLaw make_law(const femh_config& c) {
 void add_stencil_units(std::vector<StencilUnit>& out, int cellidx, const CellDesc& cd, int NT,
                        int& slot, int chunk_req = 0, int variant = 2) {
   const int R = NT / cd.nz;
-  const int maxrows = std::max(1, std::min(variant == 2 ? 2 * R - 1 : R - 1, cd.ny));
+  const bool two_rows = variant == 2 || variant == 4;
+  const int maxrows = std::max(1, std::min(two_rows ? 2 * R - 1 : R - 1, cd.ny));
   const int ntiles = (cd.ny + maxrows - 1) / maxrows;
   const int chunk = chunk_req > 0 ? std::min(chunk_req, cd.nx)
                                   : (cd.nx >= 128 ? 32 : (cd.nx >= 64 ? 16 : (cd.nx >= 16 ? 8 : cd.nx)));
@@ -424,6 +426,14 @@ void add_node_units(std::vector<NodeUnit>& out, int cellidx, long long nn, int& 
 
 template <typename T> size_t esize() { return sizeof(T); }
 
+// Threads per CTA of a stencil variant on a level: the packed two-row kernel
+// needs up to ~160 registers a thread, so it runs 384-thread CTAs where its
+// tiles still hold at least two thread rows.
+int variant_nt(int level_nt, int maxnz, int variant) {
+  if (variant == 4 && level_nt > 384 && 384 >= 2 * maxnz) return 384;
+  return level_nt;
+}
+
 }  // namespace
 
 // ======================================================== kernel launch ===
@@ -431,7 +441,19 @@ namespace {
 
 template <typename T, int NT, int OUT, int NZ, typename TIn, typename TOut, typename TB, typename TC>
 void stencil_go(femh_handle* H, dim3 grid, size_t smem, const StencilArgs<TIn, TOut, TB, TC>& a, int variant) {
-  static bool attr1 = false, attr2 = false;
+  static bool attr1 = false, attr2 = false, attr3 = false;
+  if constexpr (std::is_same<T, float>::value) {
+    if (variant == 3) {   // two load cases per CTA in packed FP32x2 lanes
+      auto fn3 = stencilp_kernel<NT, OUT, NZ, TIn, TOut, TB, TC>;
+      if (!attr3) {
+        CK(cudaFuncSetAttribute(fn3, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        attr3 = true;
+      }
+      fn3<<<dim3(grid.x, kNumRhs / 2), NT, smem, H->stream>>>(a);
+      LAUNCH_CHECK(H);
+      return;
+    }
+  }
   if (variant == 2) {
     auto fn2 = stencil2_kernel<T, NT, OUT, NZ, TIn, TOut, TB, TC>;
     if (!attr2) {
@@ -452,6 +474,19 @@ void stencil_go(femh_handle* H, dim3 grid, size_t smem, const StencilArgs<TIn, T
   LAUNCH_CHECK(H);
 }
 
+// Two voxel rows per thread in packed FP32x2 lanes (variant 4).
+template <int NT, int OUT, int NZ, typename TIn, typename TOut, typename TB, typename TC>
+void stencil_go4(femh_handle* H, dim3 grid, size_t smem, const StencilArgs<TIn, TOut, TB, TC>& a) {
+  static bool attr = false;
+  auto fn = stencil2p_kernel<NT, OUT, NZ, TIn, TOut, TB, TC>;
+  if (!attr) {
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr = true;
+  }
+  fn<<<grid, NT, smem, H->stream>>>(a);
+  LAUNCH_CHECK(H);
+}
+
 // T = arithmetic type; in/out/b storage types as given.
 template <typename T, int OUT, typename TIn, typename TOut, typename TB, typename TC>
 void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* out, const TB* b,
@@ -460,7 +495,11 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   UnitList& ul = smooth_only ? L.smooth : L.all;
   const std::vector<StencilUnit>& units = use64 ? L.su64 : ul.su;
   if (units.empty()) return;
-  const int variant = use64 ? L.variant64 : L.variant;
+  int variant = use64 ? L.variant64 : L.variant;
+  if (!std::is_same<T, float>::value) {   // packed-FP32 kernels: FP64 twin with the same units
+    if (variant == 3) variant = 1;
+    if (variant == 4) variant = 2;
+  }
   StencilArgs<TIn, TOut, TB, TC> a;
   a.cells = L.d_cells;
   a.units = use64 ? L.d_su64 : ul.d_su;
@@ -474,9 +513,16 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   a.ntot = L.ntot;
   a.k = H->hk;
   a.omega = omega;
-  const size_t smem = variant == 2
-                          ? sizeof(T) * (size_t)(2 * (6 * L.NT + 3 * L.maxnz) + 24 * L.NT) + 16 + 64 * sizeof(double)
-                          : 2 * sizeof(T) * (size_t)(15 * L.NT + 3 * L.maxnz) + 16 + 64 * sizeof(double);
+  {
+    const HadK& k = H->hk;
+    const double kv[8] = {k.A, k.Bd - k.Bo, k.Bo, k.D1 - k.O1, k.O1, k.D2 - k.O2, k.O2, k.G};
+    for (int i = 0; i < 8; ++i) a.kp[i] = make_float2((float)kv[i], (float)kv[i]);
+  }
+  const size_t smem =
+      variant == 3 ? sizeof(float4) * 12 * (size_t)L.NT + 2 * sizeof(float2) * (size_t)(12 * L.NT + 3 * L.maxnz) +
+                           64 * sizeof(double)
+      : variant == 2 ? sizeof(T) * (size_t)(2 * (6 * L.NT + 3 * L.maxnz) + 24 * L.NT) + 16 + 64 * sizeof(double)
+                     : 2 * sizeof(T) * (size_t)(15 * L.NT + 3 * L.maxnz) + 16 + 64 * sizeof(double);
   dim3 grid((unsigned)units.size(), kNumRhs);
   static const char* mode_names[] = {"apply", "apply_dot", "jacobi", "jacobi_dot", "resid"};
   char nm[64];
@@ -498,6 +544,34 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   if (OUT >= OUT_JACOBI) per += 18.0 * sizeof(TB) + (OUT == OUT_RESID ? 0.0 : 4.0);
   std::string key(nm);
   Prof prof_(H, H->prof ? H->kstats.emplace(key, femh_handle::KStat{}).first->first.c_str() : nm, nodes * per);
+  if constexpr (std::is_same<T, float>::value) {
+    if (variant == 4) {
+      const int nt = variant_nt(L.NT, L.maxnz, 4);
+      const size_t sm4 =
+          sizeof(float2) * 18 * (size_t)nt + sizeof(float) * (6 * (size_t)L.maxnz + 2) + 64 * sizeof(double);
+      if (nt == 384) {
+        switch (L.nz_spec) {
+          case 16: stencil_go4<384, OUT, 16>(H, grid, sm4, a); return;
+          case 24: stencil_go4<384, OUT, 24>(H, grid, sm4, a); return;
+          case 32: stencil_go4<384, OUT, 32>(H, grid, sm4, a); return;
+          case 48: stencil_go4<384, OUT, 48>(H, grid, sm4, a); return;
+          case 64: stencil_go4<384, OUT, 64>(H, grid, sm4, a); return;
+          case 128: stencil_go4<384, OUT, 128>(H, grid, sm4, a); return;
+          default: stencil_go4<384, OUT, 0>(H, grid, sm4, a); return;
+        }
+      }
+      if (L.nz_spec == 256) {
+        stencil_go4<512, OUT, 256>(H, grid, sm4, a);
+        return;
+      }
+      switch (nt) {
+        case 128: stencil_go4<128, OUT, 0>(H, grid, sm4, a); return;
+        case 256: stencil_go4<256, OUT, 0>(H, grid, sm4, a); return;
+        case 512: stencil_go4<512, OUT, 0>(H, grid, sm4, a); return;
+        default: throw FemhError{FEMH_E_ARG, "unsupported stencil block size"};
+      }
+    }
+  }
   switch (L.nz_spec) {   // compile-time z extent (threads fixed per extent)
     case 16: stencil_go<T, 512, OUT, 16>(H, grid, smem, a, variant); return;
     case 24: stencil_go<T, 480, OUT, 24>(H, grid, smem, a, variant); return;
@@ -559,7 +633,8 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   H->nvox = off;
   const bool mg32 = c.precision != FEMH_FP64;   // multigrid hierarchy in FP32
   const size_t vsz = mixed ? sizeof(float) : sizeof(double);   // CG vectors
-  const size_t psz = mixed ? (c.store_bf16 ? sizeof(__nv_bfloat16) : sizeof(float)) : sizeof(double);
+  const size_t psz = c.precision == FEMH_FP64 ? sizeof(double)
+                     : (c.store_bf16 ? sizeof(__nv_bfloat16) : sizeof(float));   // search directions
   const size_t msz = mg32 ? sizeof(float) : sizeof(double);
 
   // ---- levels
@@ -620,11 +695,12 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
         L.NT = (z0 == 24 || z0 == 48) ? 480 : 512;
       }
     }
+    if (c.stencil_variant > 0) L.variant = c.stencil_variant;
     int ss = 0, sn = 0;
     for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
       const CellDesc& cd = L.cells[ci];
       L.su_sb.push_back(ss);
-      add_stencil_units(L.all.su, ci, cd, L.NT, ss, 0, L.variant);
+      add_stencil_units(L.all.su, ci, cd, variant_nt(L.NT, L.maxnz, L.variant), ss, 0, L.variant);
       L.su_se.push_back(ss);
       L.nu_sb.push_back(sn);
       add_node_units(L.all.nu, ci, (long long)cd.nx * cd.ny * cd.nz, sn);
@@ -686,6 +762,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   H->cg_r = ar.get(vsz * 18 * nv);
   H->cg_p = ar.get(psz * 18 * nv);
   H->cg_q = ar.get(vsz * 18 * nv);
+  H->cg_rm = (c.precision == FEMH_MIXED_PC && gmg) ? ar.get(sizeof(float) * 18 * nv) : nullptr;
   H->d_state = ar.arr<CGState>(nc * kNumRhs);
   H->state.assign(nc * kNumRhs, CGState{});
   if (c.autotune) {
@@ -768,7 +845,7 @@ void build_stencil_units(femh_handle* H, Level& L, int chunk) {
   int ss = 0;
   for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
     L.su_sb.push_back(ss);
-    add_stencil_units(L.all.su, ci, L.cells[ci], L.NT, ss, chunk, L.variant);
+    add_stencil_units(L.all.su, ci, L.cells[ci], variant_nt(L.NT, L.maxnz, L.variant), ss, chunk, L.variant);
     L.su_se.push_back(ss);
   }
   for (auto& u : L.all.su)
@@ -866,7 +943,8 @@ void autotune_levels(femh_handle* H, bool mg) {
     Level& L = H->levels[l];
     const bool smooth = mg && l > 0;   // coarse levels only run smoothing sweeps
     if ((smooth ? L.smooth.su : L.all.su).empty()) continue;
-    std::string key = std::to_string(l) + ":" + std::to_string(L.NT) + ":" + std::to_string(sizeof(T));
+    std::string key = std::to_string(l) + ":" + std::to_string(L.NT) + ":" + std::to_string(sizeof(T)) + ":" +
+                      std::to_string(H->cfg.stencil_variant);
     int maxnx = 1;
     for (auto& cd : L.cells) {
       key += ":" + std::to_string(cd.nx) + "x" + std::to_string(cd.ny) + "x" + std::to_string(cd.nz);
@@ -892,7 +970,10 @@ void autotune_levels(femh_handle* H, bool mg) {
     std::vector<int> cands;
     for (int cand : {4, 8, 16, 32, 64, maxnx})
       if (cand <= maxnx && std::find(cands.begin(), cands.end(), cand) == cands.end()) cands.push_back(cand);
-    for (int var : {1, 2})
+    std::vector<int> vars = {1, 2};
+    if (std::is_same<T, float>::value) vars = {2, 3, 4};
+    if (H->cfg.stencil_variant > 0) vars = {H->cfg.stencil_variant};
+    for (int var : vars)
     for (int cand : cands) {
       L.variant = var;
       build_stencil_units(H, L, cand);
@@ -1002,7 +1083,7 @@ void vcycle_level_down(femh_handle* H, int l, const TB* b, TM* cur, TM* oth, TM*
   if (L.smooth.su.empty()) return;
   if (l > 0) {
     Prof prof_(H, "k_jacobi0", 0.0);
-    k_jacobi0<TB, TM><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, L.smooth.d_nu, b, cur, L.invd, om, stt,
+    k_jacobi0<TB, TM><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, L.smooth.d_nu, b, cur, (TM*)nullptr, L.invd, om, stt,
                                                           L.ntot);
     LAUNCH_CHECK(H);
   }
@@ -1091,6 +1172,7 @@ void pcg_iteration(femh_handle* H, const typename PR::K* kcg) {
   TV* r = (TV*)H->cg_r;
   TP* p = (TP*)H->cg_p;
   TV* q = (TV*)H->cg_q;
+  TM* rm = (gmg && sizeof(TM) != sizeof(TV)) ? (TM*)H->cg_rm : nullptr;
   CGState* stt = H->d_state;
   stencil<TV, OUT_APPLY_DOT>(H, L0, false, (const TP*)p, q, (const TV*)nullptr, kcg, H->d_part_s, stt, 0.0);
   {
@@ -1103,13 +1185,13 @@ void pcg_iteration(femh_handle* H, const typename PR::K* kcg) {
   {
     Prof prof_(H, "k_cg_update", 0.0);
     k_cg_update<TV, TP, TV, TM><<<NODE_GRID(L0.all), 256, 0, s>>>(
-        L0.d_cells, L0.all.d_nu, x, r, p, q, L0.invd, gmg ? (TM*)L0.xa : (TM*)nullptr, c.omega, stt,
+        L0.d_cells, L0.all.d_nu, x, r, p, q, L0.invd, gmg ? (TM*)L0.xa : (TM*)nullptr, rm, c.omega, stt,
         H->d_part_n, L0.ntot);
     LAUNCH_CHECK(H);
   }
   TM* z = nullptr;
   if (gmg) {
-    z = vcycle<TM, TMC, TV>(H, r);
+    z = rm ? vcycle<TM, TMC, TM>(H, rm) : vcycle<TM, TMC, TV>(H, r);
     Prof prof_(H, "k_dot", 0.0);
     k_dot<TM, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
     LAUNCH_CHECK(H);
@@ -1143,6 +1225,7 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
   TV* x = (TV*)H->cg_x;
   TV* r = (TV*)H->cg_r;
   TP* p = (TP*)H->cg_p;
+  TM* rm = (gmg && sizeof(TM) != sizeof(TV)) ? (TM*)H->cg_rm : nullptr;
   CGState* stt = H->d_state;
   for (auto& S : H->state) {
     S.tol = tol;
@@ -1164,11 +1247,11 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
   if (gmg) {
     {
       Prof prof_(H, "k_jacobi0", 0.0);
-      k_jacobi0<TV, TM><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, r, (TM*)L0.xa, L0.invd,
-                                                          c.omega, stt, L0.ntot);
+      k_jacobi0<TV, TM><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, r, (TM*)L0.xa, rm,
+                                                          L0.invd, c.omega, stt, L0.ntot);
       LAUNCH_CHECK(H);
     }
-    TM* z = vcycle<TM, TMC, TV>(H, r);
+    TM* z = rm ? vcycle<TM, TMC, TM>(H, rm) : vcycle<TM, TMC, TV>(H, r);
     {
       Prof prof_(H, "k_dot", 0.0);
       k_dot<TM, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
@@ -1329,8 +1412,10 @@ void solve_all(femh_handle* H, std::vector<femh_solve_info>& infos) {
     }
     if (c.precision == FEMH_FP64)
       pcg<Prec<double, double, double, double, double>>(H, H->b64, H->kc64, c.max_iter, c.tol, iters.data());
-    else   // FP64 CG and operator, FP32 multigrid preconditioner
-      pcg<Prec<double, double, double, float, float>>(H, H->b64, H->kc64, c.max_iter, c.tol, iters.data());
+    else if (c.store_bf16)   // FP64 CG and operator, FP32 multigrid, bf16 search directions
+      pcg<Prec<double, __nv_bfloat16, double, float, float>>(H, H->b64, H->kc64, c.max_iter, c.tol, iters.data());
+    else   // FP64 CG and operator, FP32 multigrid preconditioner and search directions
+      pcg<Prec<double, float, double, float, float>>(H, H->b64, H->kc64, c.max_iter, c.tol, iters.data());
     for (int t = 0; t < nc * kNumRhs; ++t) final_status[t] = H->state[t].status;
     outer_done = 1;
     true_residual(H, rn2);
@@ -1528,6 +1613,7 @@ femh_status femh_config_default(femh_config* c) {
   c->graph_chunk = 8;
   c->coarse_avg = 0;
   c->autotune = 1;
+  c->stencil_variant = 0;
   return FEMH_OK;
 }
 
@@ -1758,10 +1844,17 @@ femh_status femh_apply_operator(femh_handle* H, int nx, int ny, int nz, double h
     CK(cudaMemcpyAsync(H->rho_in, rho, sizeof(double) * nn, k_in, s));
     Level& L0 = H->levels[0];
     const MatLaw law = make_law(H->cfg);
+    // FP32 operator (the arithmetic of the mixed modes' multigrid sweeps) when
+    // the handle is configured for a mixed precision with FP32 storage
+    const bool f32 = H->cfg.precision != FEMH_FP64 && !H->cfg.store_bf16;
     {
       Prof prof_(H, "k_coef", 0.0);
-      k_coef<double><<<(unsigned)L0.all.nu.size(), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->rho_in, law, H->kc64,
-                                                              (double*)nullptr, H->rho_used);
+      if (f32)
+        k_coef<float><<<(unsigned)L0.all.nu.size(), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->rho_in, law, H->kc64,
+                                                               (float*)L0.kc, H->rho_used);
+      else
+        k_coef<double><<<(unsigned)L0.all.nu.size(), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->rho_in, law,
+                                                                H->kc64, (double*)nullptr, H->rho_used);
       LAUNCH_CHECK(H);
     }
     double* tmp = H->d_out;
@@ -1771,8 +1864,21 @@ femh_status femh_apply_operator(femh_handle* H, int nx, int ny, int nz, double h
       k_layout<false><<<cdiv(18 * nn, 256), 256, 0, s>>>(tmp, H->x64, 0, nn, L0.ntot);
       LAUNCH_CHECK(H);
     }
-    stencil<double, OUT_APPLY>(H, L0, false, (const double*)H->x64, H->b64, (const double*)nullptr,
-                               (const double*)H->kc64, nullptr, nullptr, 0.0);
+    if (f32) {
+      float* uf = (float*)H->cg_r;
+      float* yf = (float*)H->cg_q;
+      k_copy<float, double><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, uf, H->x64, nullptr,
+                                                              L0.ntot);
+      LAUNCH_CHECK(H);
+      stencil<float, OUT_APPLY>(H, L0, false, (const float*)uf, yf, (const float*)nullptr, (const float*)L0.kc,
+                                nullptr, nullptr, 0.0);
+      k_copy<double, float><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->b64, yf, nullptr,
+                                                              L0.ntot);
+      LAUNCH_CHECK(H);
+    } else {
+      stencil<double, OUT_APPLY>(H, L0, false, (const double*)H->x64, H->b64, (const double*)nullptr,
+                                 (const double*)H->kc64, nullptr, nullptr, 0.0);
+    }
     {
       Prof prof_(H, "k_layout", 0.0);
       k_layout<true><<<cdiv(18 * nn, 256), 256, 0, s>>>(H->b64, tmp, 0, nn, L0.ntot);

@@ -188,10 +188,13 @@ __global__ void k_cg_init(const CellDesc* cells, const NodeUnit* units, const TB
 
 // x += alpha p ; r -= alpha q (r = 0 at node 0) ; partial ||r||^2 and, for
 // Jacobi, r.(invd r).  For the multigrid preconditioner (z0 != nullptr) it
-// also writes the first damped-Jacobi sweep from zero: z0 = omega invd r.
+// also writes the first damped-Jacobi sweep from zero: z0 = omega invd r, and,
+// when rm != nullptr, r in the V-cycle's storage type (the level-0 right-hand
+// side its sweeps read).
 template <typename TV, typename TP, typename TQ, typename TZ>
 __global__ void k_cg_update(const CellDesc* cells, const NodeUnit* units, TV* __restrict__ x, TV* __restrict__ r, const TP* __restrict__ p,
-                            const TQ* __restrict__ q, const float* __restrict__ invd, TZ* __restrict__ z0, double omega, const CGState* stt,
+                            const TQ* __restrict__ q, const float* __restrict__ invd, TZ* __restrict__ z0,
+                            TZ* __restrict__ rm, double omega, const CGState* stt,
                             double* __restrict__ part, long long ntot) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
@@ -215,6 +218,7 @@ __global__ void k_cg_update(const CellDesc* cells, const NodeUnit* units, TV* __
         v[0] += rv * rv;
         v[1] += rv * id * rv;
         if (z0) st_val(z0 + o, omega * id * rv);
+        if (rm) st_val(rm + o, rv);
       }
     }
   }
@@ -453,10 +457,12 @@ __global__ void k_prolong_add(const CellDesc* __restrict__ fine, const CellDesc*
   }
 }
 
-// z = omega * invd * b  (first damped-Jacobi sweep from a zero start)
+// z = omega * invd * b  (first damped-Jacobi sweep from a zero start); with
+// bcopy != nullptr also b converted to TX.
 template <typename TB, typename TX>
 __global__ void k_jacobi0(const CellDesc* cells, const NodeUnit* units, const TB* __restrict__ b, TX* __restrict__ x,
-                          const float* __restrict__ invd, double omega, const CGState* stt, long long ntot) {
+                          TX* __restrict__ bcopy, const float* __restrict__ invd, double omega, const CGState* stt,
+                          long long ntot) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cd = cells[u.cell];
@@ -468,7 +474,9 @@ __global__ void k_jacobi0(const CellDesc* cells, const NodeUnit* units, const TB
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long o = ((long long)rhs * 3 + c) * ntot + g;
-      st_val(x + o, omega * id * (double)ld_val(b + o));
+      const double bv = (double)ld_val(b + o);
+      st_val(x + o, omega * id * bv);
+      if (bcopy) st_val(bcopy + o, bv);
     }
   }
 }

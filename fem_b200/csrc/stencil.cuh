@@ -48,6 +48,7 @@ struct StencilArgs {
   long long ntot;        // nodes of the level over all cells
   HadK k;
   double omega;
+  float2 kp[8];          // FP32 pairs (x = y) of A, Bd-Bo, Bo, D1-O1, O1, D2-O2, O2, G
 };
 
 template <typename T>
@@ -580,6 +581,646 @@ stencil2_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
     block_reduce<1>(v, red);
     if (tid == 0) a.partials[(long long)un.slot * kNumRhs + rhs] = v[0];
   }
+}
+
+// ------------------------------------------------------------------ pairs ---
+// Two load cases of one node or voxel in the two lanes of a packed FP32x2
+// register: sm_100 add/sub/mul/fma.f32x2 process both lanes in one
+// instruction, and the two cases share every index, coefficient and shared
+// memory access (64-bit).
+using f2 = float2;
+__device__ __forceinline__ f2 p_add(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 p_mul(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 p_fma(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ f2 p_sub(f2 a, f2 b) {
+  unsigned long long ra, rb, rd;
+  memcpy(&ra, &a, 8);
+  memcpy(&rb, &b, 8);
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(rd) : "l"(ra), "l"(rb));
+  f2 d;
+  memcpy(&d, &rd, 8);
+  return d;
+}
+__device__ __forceinline__ f2 p_bc(float s) { return make_float2(s, s); }
+
+// 2x2 Hadamard transform of a node patch, index 2*ay + az (same stage order
+// and signs as fwht8_fwd restricted to bits 1 and 2).
+__device__ __forceinline__ void had4_fwd(f2 (&v)[4]) {
+  const f2 a0 = p_add(v[1], v[0]), a1 = p_sub(v[1], v[0]);
+  const f2 a2 = p_add(v[3], v[2]), a3 = p_sub(v[3], v[2]);
+  v[0] = p_add(a2, a0);
+  v[2] = p_sub(a2, a0);
+  v[1] = p_add(a3, a1);
+  v[3] = p_sub(a3, a1);
+}
+// Inverse stages of fwht8_inv for bits 2 and 1.
+__device__ __forceinline__ void had4_inv(f2 (&v)[4]) {
+  const f2 a0 = p_sub(v[0], v[2]), a2 = p_add(v[0], v[2]);
+  const f2 a1 = p_sub(v[1], v[3]), a3 = p_add(v[1], v[3]);
+  v[0] = p_sub(a0, a1);
+  v[1] = p_add(a0, a1);
+  v[2] = p_sub(a2, a3);
+  v[3] = p_add(a2, a3);
+}
+
+// had_block on packed pairs; s = c_e * h (one scale for both lanes).
+__device__ __forceinline__ void had_block_p(f2 (&w)[3][8], const HadK& K, float s) {
+  const f2 A = p_bc(s * (float)K.A), Bdo = p_bc(s * (float)(K.Bd - K.Bo)), Bo = p_bc(s * (float)K.Bo);
+  const f2 D1o = p_bc(s * (float)(K.D1 - K.O1)), O1 = p_bc(s * (float)K.O1);
+  const f2 D2o = p_bc(s * (float)(K.D2 - K.O2)), O2 = p_bc(s * (float)K.O2), G = p_bc(s * (float)K.G);
+  {
+    const f2 n0 = w[0][4], n1 = w[1][2], n2 = w[2][1];
+    const f2 t = p_mul(Bo, p_add(p_add(n0, n1), n2));
+    w[0][4] = p_fma(Bdo, n0, t);
+    w[1][2] = p_fma(Bdo, n1, t);
+    w[2][1] = p_fma(Bdo, n2, t);
+  }
+  {
+    const f2 sxz = p_mul(A, p_add(w[0][1], w[2][4]));
+    const f2 syz = p_mul(A, p_add(w[1][1], w[2][2]));
+    const f2 sxy = p_mul(A, p_add(w[0][2], w[1][4]));
+    w[0][1] = sxz; w[2][4] = sxz;
+    w[1][1] = syz; w[2][2] = syz;
+    w[0][2] = sxy; w[1][4] = sxy;
+  }
+  {
+    const f2 t0 = w[0][3], t1 = w[1][5], t2 = w[2][6];
+    const f2 t = p_mul(O1, p_add(p_add(t0, t1), t2));
+    w[0][3] = p_fma(D1o, t0, t);
+    w[1][5] = p_fma(D1o, t1, t);
+    w[2][6] = p_fma(D1o, t2, t);
+  }
+  {
+    const f2 a = w[1][3], b = w[0][5], t = p_mul(O2, p_add(a, b));
+    w[1][3] = p_fma(D2o, a, t); w[0][5] = p_fma(D2o, b, t);
+  }
+  {
+    const f2 a = w[2][3], b = w[0][6], t = p_mul(O2, p_add(a, b));
+    w[2][3] = p_fma(D2o, a, t); w[0][6] = p_fma(D2o, b, t);
+  }
+  {
+    const f2 a = w[2][5], b = w[1][6], t = p_mul(O2, p_add(a, b));
+    w[2][5] = p_fma(D2o, a, t); w[1][6] = p_fma(D2o, b, t);
+  }
+  w[0][7] = p_mul(w[0][7], G); w[1][7] = p_mul(w[1][7], G); w[2][7] = p_mul(w[2][7], G);
+}
+
+// One voxel row per thread, two load cases per CTA (blockIdx.y = case pair),
+// FP32x2 arithmetic.  Layout and schedule of stencil_kernel, with two changes
+// that remove redundant transform work: the lower node plane of each voxel is
+// carried from the previous step already transformed in y and z (a voxel's
+// upper plane is the next voxel's lower plane), and the upper-plane
+// contributions are carried in the same half-transformed basis, so the y/z
+// inverse stages run once per node plane on the summed contributions of both
+// voxels that share it.  Shared memory: P[2][R+1][3][nz] node planes and
+// Q[2][R][3 corners][3][nz] corner totals (pairs, shared between threads), and
+// per thread the two carried sets (12 pairs each) as float4 slots
+// [6][NT] that only their thread touches (no barrier; registers stay below
+// the 128 a 512-thread CTA allows).
+template <int NT, int OUT, int NZ, typename TIn, typename TOut, typename TB, typename TC>
+__global__ void __launch_bounds__(NT, 1)
+stencilp_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const StencilUnit un = a.units[blockIdx.x];
+  const int pr = blockIdx.y;   // load cases 2pr, 2pr+1
+  const CellDesc cd = a.cells[un.cell];
+  if (a.stt && !a.stt[cd.id * kNumRhs + 2 * pr].active && !a.stt[cd.id * kNumRhs + 2 * pr + 1].active) return;
+  const int nx = cd.nx, ny = cd.ny;
+  const int nz = NZ > 0 ? NZ : cd.nz;
+  const int R = NT / nz;
+  const int tid = threadIdx.x;
+  const int r = tid / nz, z = tid - r * nz;
+  const bool live = r < R && r <= un.rows;
+  const int zp = (z + 1 == nz) ? 0 : z + 1;
+  const int zm = (z == 0) ? nz - 1 : z - 1;
+  int jr = un.j0 - 1 + r;
+  if (jr < 0) jr += ny;
+  while (jr >= ny) jr -= ny;
+  const int jr1 = (jr + 1 == ny) ? 0 : jr + 1;
+  const bool extra = live && r == un.rows;
+  const bool owner = live && r >= 1;
+
+  // private carries first (16-byte aligned float4 slots), then P, Q, reduction
+  float4* CPv = reinterpret_cast<float4*>(smem_raw);   // [6][NT] transformed lower plane
+  float4* CCa = CPv + 6 * NT;                           // [6][NT] upper-plane contributions
+  const int PS = (R + 1) * 3 * nz;   // pairs in one P buffer
+  const int QS = R * 9 * nz;         // pairs in one Q buffer
+  f2* P = reinterpret_cast<f2*>(CCa + 6 * NT);
+  f2* Q = P + 2 * PS;
+  double* red = reinterpret_cast<double*>(Q + 2 * QS);
+  const int prow = r * 3 * nz, qrow = r * 9 * nz;
+  const int qup = (r > 0 ? r - 1 : 0) * 9 * nz;
+
+  const long long st = a.ntot, st3 = 3 * a.ntot;
+  const int plane = ny * nz;
+  const int cellsz = nx * plane;
+  const int col0 = jr * nz + z, col1 = jr1 * nz + z;
+  const TIn* ua = a.u + (long long)(2 * pr) * 3 * st + cd.off;
+  const TC* kcb = a.kc + cd.off + col0;
+  const TB* ba = (OUT >= OUT_JACOBI) ? a.b + (long long)(2 * pr) * 3 * st + cd.off + col0 : nullptr;
+  const float* ib = a.invd + cd.off + col0;
+  TOut* oa = a.out + (long long)(2 * pr) * 3 * st + cd.off + col0;
+
+  auto ldp = [&](const TIn* p) { return make_float2((float)ld_val(p), (float)ld_val(p + st3)); };
+  auto put = [&](float4* base, const f2 (&h)[3][4]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+        base[(2 * c + k) * NT + tid] = make_float4(h[c][2 * k].x, h[c][2 * k].y, h[c][2 * k + 1].x, h[c][2 * k + 1].y);
+  };
+  auto get = [&](const float4* base, f2 (&h)[3][4]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const float4 v = base[(2 * c + k) * NT + tid];
+        h[c][2 * k] = make_float2(v.x, v.y);
+        h[c][2 * k + 1] = make_float2(v.z, v.w);
+      }
+  };
+
+  using TBv = decltype(ld_val(a.b));   // raw operand, converted where it is used
+  f2 ld0[3], ld1[3];
+  TBv ebA[3], ebB[3];
+  float kcv = 0.f, kc_next = 0.f, eid = 0.f;
+  f2 own[3], unode[3], rawn[3];
+  int pg = 0;
+  double accA = 0.0, accB = 0.0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    ld0[c] = ld1[c] = own[c] = unode[c] = rawn[c] = p_bc(0.f);
+    ebA[c] = ebB[c] = (TBv)0;
+  }
+
+  auto adv = [&](int& o) { o += plane; if (o >= cellsz) o -= cellsz; };
+  auto gather = [&](const f2* Qg) {
+    f2 y[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      y[c] = p_add(p_add(own[c], Qg[qrow + (0 * 3 + c) * nz + zm]),
+                   p_add(Qg[qup + (1 * 3 + c) * nz + z], Qg[qup + (2 * 3 + c) * nz + zm]));
+    TOut* ob = oa + pg;
+    if (OUT == OUT_APPLY || OUT == OUT_APPLY_DOT) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        st_val(ob + c * st, y[c].x);
+        st_val(ob + c * st + st3, y[c].y);
+        if (OUT == OUT_APPLY_DOT) {
+          accA += (double)unode[c].x * (double)y[c].x;
+          accB += (double)unode[c].y * (double)y[c].y;
+        }
+      }
+    } else {
+      const bool pin = (pg + col0 == 0);
+      const f2 wd = p_bc((float)a.omega * eid);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const f2 bv = make_float2((float)ebA[c], (float)ebB[c]);
+        const f2 d = p_sub(bv, y[c]);
+        if (OUT == OUT_RESID) {
+          st_val(ob + c * st, pin ? 0.f : d.x);
+          st_val(ob + c * st + st3, pin ? 0.f : d.y);
+        } else {
+          const f2 xv = p_fma(wd, d, unode[c]);
+          st_val(ob + c * st, xv.x);
+          st_val(ob + c * st + st3, xv.y);
+          if (OUT == OUT_JACOBI_DOT) {
+            accA += (double)xv.x * (double)bv.x;
+            accB += (double)xv.y * (double)bv.y;
+          }
+        }
+      }
+    }
+  };
+  // the 2x2 patch of node plane Pb whose lower corner is this thread's node
+  // (own value given), transformed in y and z
+  auto patch = [&](const f2* Pb, const f2 (&mine)[3], f2 (&h)[3][4]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      h[c][0] = mine[c];
+      h[c][1] = Pb[prow + c * nz + zp];
+      h[c][2] = Pb[prow + (3 + c) * nz + z];
+      h[c][3] = Pb[prow + (3 + c) * nz + zp];
+      had4_fwd(h[c]);
+    }
+  };
+
+  // prologue: node plane i0-1 -> carried lower plane (through P[1])
+  int pk = ((un.i0 - 1 + nx) % nx) * plane;
+  int pn = pk;
+  if (live) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      ld0[c] = ldp(ua + c * st + pn + col0);
+      if (extra) ld1[c] = ldp(ua + c * st + pn + col1);
+    }
+    kc_next = (float)ld_val(kcb + pk);
+    f2* Pw = P + PS;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Pw[prow + c * nz + z] = ld0[c];
+      if (extra) Pw[prow + (3 + c) * nz + z] = ld1[c];
+    }
+  }
+  __syncthreads();
+  adv(pn);
+  if (live) {
+    f2 h[3][4];
+    patch(P + PS, ld0, h);
+    put(CPv, h);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) h[c][q] = p_bc(0.f);
+      rawn[c] = ld0[c];
+      ld0[c] = ldp(ua + c * st + pn + col0);
+      if (extra) ld1[c] = ldp(ua + c * st + pn + col1);
+    }
+    put(CCa, h);
+  }
+
+  for (int s = 0; s <= un.len; ++s) {
+    const int pe = pk;   // voxel plane ie = i0-1+s; node plane ie+1 is in ld0/ld1
+    f2* Pb = P + (s & 1) * PS;
+    f2* Qb = Q + (s & 1) * QS;
+    f2 cur0[3];
+    if (live) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        Pb[prow + c * nz + z] = ld0[c];
+        if (extra) Pb[prow + (3 + c) * nz + z] = ld1[c];
+        cur0[c] = ld0[c];
+      }
+      kcv = kc_next;
+      if (s < un.len) {
+        adv(pn);
+        adv(pk);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          ld0[c] = ldp(ua + c * st + pn + col0);
+          if (extra) ld1[c] = ldp(ua + c * st + pn + col1);
+        }
+        kc_next = (float)ld_val(kcb + pk);
+      }
+    }
+    __syncthreads();   // P[s&1] holds node plane ie+1; Q[(s-1)&1] holds node plane ie-1
+    if (s >= 2 && owner) gather(Q + ((s - 1) & 1) * QS);
+    if (OUT >= OUT_JACOBI && owner && s >= 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ebA[c] = ld_val(ba + c * st + pe);
+        ebB[c] = ld_val(ba + c * st + st3 + pe);
+      }
+      if (OUT != OUT_RESID) eid = ib[pe];
+    }
+    if (live) {
+      f2 w[3][8];
+      {
+        f2 cur[3][4], prv[3][4];
+        patch(Pb, cur0, cur);
+        get(CPv, prv);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            if (q > 0) w[c][q] = p_add(cur[c][q], prv[c][q]);
+            w[c][4 + q] = p_sub(cur[c][q], prv[c][q]);
+          }
+        put(CPv, cur);
+      }
+      had_block_p(w, a.k, kcv);
+      // inverse x stage: lower plane (node plane ie) = w[q] - w[4+q], upper
+      // plane = w[q] + w[4+q]; w[0] = 0 (translations carry no energy)
+      f2 car[3][4];
+      get(CCa, car);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        f2 tot[4];
+        tot[0] = p_sub(car[c][0], w[c][4]);
+        car[c][0] = w[c][4];
+#pragma unroll
+        for (int q = 1; q < 4; ++q) {
+          tot[q] = p_add(p_sub(w[c][q], w[c][4 + q]), car[c][q]);
+          car[c][q] = p_add(w[c][q], w[c][4 + q]);
+        }
+        had4_inv(tot);
+        own[c] = tot[0];
+        unode[c] = rawn[c];
+        rawn[c] = cur0[c];
+        if (s > 0) {
+          Qb[qrow + (0 * 3 + c) * nz + z] = tot[1];   // node (jr, z+1)
+          Qb[qrow + (1 * 3 + c) * nz + z] = tot[2];   // node (jr+1, z)
+          Qb[qrow + (2 * 3 + c) * nz + z] = tot[3];   // node (jr+1, z+1)
+        }
+      }
+      put(CCa, car);
+      pg = pe;
+    }
+  }
+  __syncthreads();
+  if (un.len >= 1 && owner) gather(Q + (un.len & 1) * QS);
+
+  if (OUT == OUT_APPLY_DOT || OUT == OUT_JACOBI_DOT) {
+    double v[2] = {accA, accB};
+    block_reduce<2>(v, red);
+    if (tid == 0) {
+      a.partials[(long long)un.slot * kNumRhs + 2 * pr] = v[0];
+      a.partials[(long long)un.slot * kNumRhs + 2 * pr + 1] = v[1];
+    }
+  }
+}
+
+// Two voxel rows per thread with the two voxels in the two lanes of packed
+// FP32x2 registers (FP32 operators).  Thread (t, z) streams voxels (i, e0, z)
+// (lane x) and (i, e0+1, z) (lane y), e0 = j0-1+2t, along x; node rows
+// n0 = e0, n1, n2.  Lane x of a patch pair is row n0 or n1 and lane y the row
+// one above, so the pair (n1, n2) of this thread's own nodes is used as
+// loaded, and the two stiffness scales (kc of rows e0, e0+1) form a pair.  As
+// in stencilp_kernel the lower node plane is carried transformed in y and z
+// and the upper-plane contributions are carried half transformed.
+// Shared memory (double-buffered): P2[TR][3][nz] pairs (n1, n2) of each
+// thread, H0[3][nz] the halo row n0 of thread 0; QAB[TR][3][nz] pairs of
+// corner totals (node (n1, z+1), node (n2, z+1)) and QCD[TR][3][nz] pairs
+// (node (n0, z), node (n0, z+1)) for the thread below.
+template <int NT, int OUT, int NZ, typename TIn, typename TOut, typename TB, typename TC>
+__global__ void __launch_bounds__(NT, 1)
+stencil2p_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const StencilUnit un = a.units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cd = a.cells[un.cell];
+  if (a.stt && !a.stt[cd.id * kNumRhs + rhs].active) return;
+  const int nx = cd.nx, ny = cd.ny;
+  const int nz = NZ > 0 ? NZ : cd.nz;
+  const int TR = NT / nz;
+  const int tid = threadIdx.x;
+  const int t = tid / nz, z = tid - t * nz;
+  const int rows = un.rows;
+  const bool live = t < TR && 2 * t <= rows;
+  const bool own1 = live && 2 * t < rows;
+  const bool own2 = live && 2 * t + 1 < rows;
+  const int zp = (z + 1 == nz) ? 0 : z + 1;
+  const int zm = (z == 0) ? nz - 1 : z - 1;
+  auto wrapy = [&](int j) { j %= ny; return j < 0 ? j + ny : j; };
+  const int n0 = wrapy(un.j0 - 1 + 2 * t), n1 = wrapy(n0 + 1), n2 = wrapy(n0 + 2);
+
+  const int PS = TR * 3 * nz;        // pairs in one P2 / QAB / QCD buffer
+  f2* P2 = reinterpret_cast<f2*>(smem_raw);   // [2][TR][3][nz]
+  f2* QAB = P2 + 2 * PS;                       // [2][TR][3][nz]
+  f2* QCD = QAB + 2 * PS;                      // [2][TR][3][nz]
+  float* H0 = reinterpret_cast<float*>(QCD + 2 * PS);   // [2][3][nz]
+  double* red = reinterpret_cast<double*>(H0 + ((6 * nz + 1) & ~1));
+  const int pt = t * 3 * nz;                   // this thread's slot
+  const int pb = (t > 0 ? t - 1 : 0) * 3 * nz; // slot of the thread below (n0 = its n2)
+  const int pa = (t + 1 < TR ? t + 1 : t) * 3 * nz;   // slot of the thread above
+
+  const long long st = a.ntot;
+  const int plane = ny * nz;
+  const int cellsz = nx * plane;
+  const int c0 = n0 * nz + z, c1 = n1 * nz + z, c2 = n2 * nz + z;
+  const TIn* ub = a.u + (long long)rhs * 3 * st + cd.off;
+  const TC* kcb = a.kc + cd.off;
+  const TB* bb = (OUT >= OUT_JACOBI) ? a.b + (long long)rhs * 3 * st + cd.off : nullptr;
+  const float* ib = a.invd + cd.off;
+  TOut* obase = a.out + (long long)rhs * 3 * st + cd.off;
+
+  using TBv = decltype(ld_val(a.b));
+  f2 l12[3];                 // node plane being prefetched: rows (n1, n2)
+  float l0[3] = {0.f, 0.f, 0.f};   // and row n0 (thread 0: the halo row)
+  f2 kn = p_bc(0.f), kv;     // kc of voxel rows (e0, e0+1), next and current
+  f2 prv[3][4], car[3][4];
+  f2 own[3], u12[3], raw[3];
+  TBv eb1[3], eb2[3];
+  f2 id12 = p_bc(0.f);
+  int pg = 0;
+  double acc = 0.0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    l12[c] = own[c] = u12[c] = raw[c] = p_bc(0.f);
+    eb1[c] = eb2[c] = (TBv)0;
+  }
+
+  auto adv = [&](int& o) { o += plane; if (o >= cellsz) o -= cellsz; };
+  auto load_plane = [&](int po) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (t == 0) l0[c] = (float)ld_val(ub + c * st + po + c0);
+      l12[c] = make_float2((float)ld_val(ub + c * st + po + c1), (float)ld_val(ub + c * st + po + c2));
+    }
+  };
+  auto load_kc = [&](int pk) { kn = make_float2((float)ld_val(kcb + pk + c0), (float)ld_val(kcb + pk + c1)); };
+  auto store_plane = [&](f2* Pb, float* Hb) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Pb[pt + c * nz + z] = l12[c];
+      if (t == 0) Hb[c * nz + z] = l0[c];
+    }
+  };
+  // y/z-transformed patches of the node plane in Pb/Hb (own pair given)
+  auto patch = [&](const f2* Pb, const float* Hb, const f2 (&mine)[3], f2 (&h)[3][4]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const f2 up = Pb[pt + c * nz + zp];   // (n1, n2) at z+1
+      const float b0 = t == 0 ? Hb[c * nz + z] : Pb[pb + c * nz + z].y;
+      const float b1 = t == 0 ? Hb[c * nz + zp] : Pb[pb + c * nz + zp].y;
+      h[c][0] = make_float2(b0, mine[c].x);
+      h[c][1] = make_float2(b1, up.x);
+      h[c][2] = mine[c];
+      h[c][3] = up;
+      had4_fwd(h[c]);
+    }
+  };
+  auto epilogue = [&](const f2 (&y)[3]) {
+    TOut* ob = obase + pg;
+    if (OUT == OUT_APPLY || OUT == OUT_APPLY_DOT) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (own1) st_val(ob + c * st + c1, y[c].x);
+        if (own2) st_val(ob + c * st + c2, y[c].y);
+        if (OUT == OUT_APPLY_DOT) {
+          if (own1) acc += (double)u12[c].x * (double)y[c].x;
+          if (own2) acc += (double)u12[c].y * (double)y[c].y;
+        }
+      }
+    } else {
+      const bool pin1 = (pg + c1 == 0), pin2 = (pg + c2 == 0);
+      const f2 wd = p_mul(p_bc((float)a.omega), id12);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const f2 bv = make_float2((float)eb1[c], (float)eb2[c]);
+        const f2 d = p_sub(bv, y[c]);
+        if (OUT == OUT_RESID) {
+          if (own1) st_val(ob + c * st + c1, pin1 ? 0.f : d.x);
+          if (own2) st_val(ob + c * st + c2, pin2 ? 0.f : d.y);
+        } else {
+          const f2 xv = p_fma(wd, d, u12[c]);
+          if (own1) st_val(ob + c * st + c1, xv.x);
+          if (own2) st_val(ob + c * st + c2, xv.y);
+          if (OUT == OUT_JACOBI_DOT) {
+            if (own1) acc += (double)xv.x * (double)bv.x;
+            if (own2) acc += (double)xv.y * (double)bv.y;
+          }
+        }
+      }
+    }
+  };
+  auto gather = [&](int buf) {
+    const f2* Qab = QAB + buf * PS;
+    const f2* Qcd = QCD + buf * PS;
+    f2 y[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      y[c] = p_add(own[c], Qab[pt + c * nz + zm]);
+      y[c].y += Qcd[pa + c * nz + z].x + Qcd[pa + c * nz + zm].y;
+    }
+    epilogue(y);
+  };
+
+  // prologue: node plane i0-1 -> carried transformed patches (through buffer 1)
+  int pk = ((un.i0 - 1 + nx) % nx) * plane;
+  int pn = pk;
+  if (live) {
+    load_plane(pn);
+    load_kc(pk);
+    store_plane(P2 + PS, H0 + 3 * nz);
+  }
+  __syncthreads();
+  adv(pn);
+  if (live) {
+    patch(P2 + PS, H0 + 3 * nz, l12, prv);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      raw[c] = l12[c];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) car[c][q] = p_bc(0.f);
+    }
+    load_plane(pn);
+  }
+
+  for (int s = 0; s <= un.len; ++s) {
+    const int pe = pk;   // voxel plane ie = i0-1+s; node plane ie+1 is in l12/l0
+    const int buf = s & 1;
+    f2* Pb = P2 + buf * PS;
+    float* Hb = H0 + buf * 3 * nz;
+    f2 cur0[3];
+    if (live) {
+      store_plane(Pb, Hb);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) cur0[c] = l12[c];
+      kv = kn;
+      if (s < un.len) {
+        adv(pn);
+        adv(pk);
+        load_plane(pn);
+        load_kc(pk);
+      }
+    }
+    __syncthreads();   // buffer buf holds node plane ie+1; Q[buf^1] holds node plane ie-1
+    if (s >= 2 && live) gather(buf ^ 1);
+    if (OUT >= OUT_JACOBI && s >= 1 && live) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        eb1[c] = ld_val(bb + c * st + pe + c1);
+        eb2[c] = ld_val(bb + c * st + pe + c2);
+      }
+      if (OUT != OUT_RESID) id12 = make_float2(ib[pe + c1], ib[pe + c2]);
+    }
+    if (live) {
+      f2 w[3][8];
+      {
+        f2 cur[3][4];
+        patch(Pb, Hb, cur0, cur);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            if (q > 0) w[c][q] = p_add(cur[c][q], prv[c][q]);
+            w[c][4 + q] = p_sub(cur[c][q], prv[c][q]);
+            prv[c][q] = cur[c][q];
+          }
+      }
+      {   // Hadamard-domain element operator, scales (kc(e0), kc(e0+1))
+        const f2 A = p_mul(kv, a.kp[0]), Bdo = p_mul(kv, a.kp[1]), Bo = p_mul(kv, a.kp[2]);
+        const f2 D1o = p_mul(kv, a.kp[3]), O1 = p_mul(kv, a.kp[4]);
+        const f2 D2o = p_mul(kv, a.kp[5]), O2 = p_mul(kv, a.kp[6]), G = p_mul(kv, a.kp[7]);
+        {
+          const f2 m0 = w[0][4], m1 = w[1][2], m2 = w[2][1];
+          const f2 tt = p_mul(Bo, p_add(p_add(m0, m1), m2));
+          w[0][4] = p_fma(Bdo, m0, tt); w[1][2] = p_fma(Bdo, m1, tt); w[2][1] = p_fma(Bdo, m2, tt);
+        }
+        {
+          const f2 sxz = p_mul(A, p_add(w[0][1], w[2][4]));
+          const f2 syz = p_mul(A, p_add(w[1][1], w[2][2]));
+          const f2 sxy = p_mul(A, p_add(w[0][2], w[1][4]));
+          w[0][1] = sxz; w[2][4] = sxz; w[1][1] = syz; w[2][2] = syz; w[0][2] = sxy; w[1][4] = sxy;
+        }
+        {
+          const f2 m0 = w[0][3], m1 = w[1][5], m2 = w[2][6];
+          const f2 tt = p_mul(O1, p_add(p_add(m0, m1), m2));
+          w[0][3] = p_fma(D1o, m0, tt); w[1][5] = p_fma(D1o, m1, tt); w[2][6] = p_fma(D1o, m2, tt);
+        }
+        {
+          const f2 x0 = w[1][3], x1 = w[0][5], tt = p_mul(O2, p_add(x0, x1));
+          w[1][3] = p_fma(D2o, x0, tt); w[0][5] = p_fma(D2o, x1, tt);
+        }
+        {
+          const f2 x0 = w[2][3], x1 = w[0][6], tt = p_mul(O2, p_add(x0, x1));
+          w[2][3] = p_fma(D2o, x0, tt); w[0][6] = p_fma(D2o, x1, tt);
+        }
+        {
+          const f2 x0 = w[2][5], x1 = w[1][6], tt = p_mul(O2, p_add(x0, x1));
+          w[2][5] = p_fma(D2o, x0, tt); w[1][6] = p_fma(D2o, x1, tt);
+        }
+        w[0][7] = p_mul(w[0][7], G); w[1][7] = p_mul(w[1][7], G); w[2][7] = p_mul(w[2][7], G);
+      }
+      f2* Qab = QAB + buf * PS;
+      f2* Qcd = QCD + buf * PS;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        f2 tot[4];
+        tot[0] = p_sub(car[c][0], w[c][4]);
+        car[c][0] = w[c][4];
+#pragma unroll
+        for (int q = 1; q < 4; ++q) {
+          tot[q] = p_add(p_sub(w[c][q], w[c][4 + q]), car[c][q]);
+          car[c][q] = p_add(w[c][q], w[c][4 + q]);
+        }
+        had4_inv(tot);
+        // lane x: rows (n0 | n1), lane y: rows (n1 | n2); index 2*ay + az
+        own[c] = make_float2(tot[0].y + tot[2].x, tot[2].y);   // nodes (n1, z), (n2, z)
+        u12[c] = raw[c];
+        raw[c] = cur0[c];
+        if (s > 0) {
+          Qab[pt + c * nz + z] = make_float2(tot[1].y + tot[3].x, tot[3].y);   // (n1, z+1), (n2, z+1)
+          Qcd[pt + c * nz + z] = make_float2(tot[0].x, tot[1].x);             // (n0, z), (n0, z+1)
+        }
+      }
+      pg = pe;
+    }
+  }
+  __syncthreads();
+  if (un.len >= 1 && live) gather(un.len & 1);
+
+  if (OUT == OUT_APPLY_DOT || OUT == OUT_JACOBI_DOT) {
+    double v[1] = {acc};
+    block_reduce<1>(v, red);
+    if (tid == 0) a.partials[(long long)un.slot * kNumRhs + rhs] = v[0];
+  }
+}
+
+// Shared memory bytes of one stencil2p_kernel CTA.
+inline size_t stencil2p_smem_bytes(int NT, int nz) {
+  const int TR = NT / nz;
+  return sizeof(f2) * 6 * (size_t)TR * 3 * nz + sizeof(float) * ((6 * (size_t)nz + 1) & ~(size_t)1) +
+         64 * sizeof(double);
+}
+
+// Shared memory bytes of one pair-kernel CTA.
+inline size_t stencilp_smem_bytes(int NT, int nz) {
+  const int R = NT / nz;
+  return sizeof(float4) * 12 * (size_t)NT + sizeof(f2) * 2 * ((size_t)(R + 1) * 3 * nz + (size_t)R * 9 * nz) +
+         64 * sizeof(double);
 }
 
 }  // namespace femh

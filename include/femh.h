@@ -79,6 +79,10 @@ typedef struct {
   int coarse_avg;         /* coarse voxel modulus from its 8 children: 0 arithmetic mean
                              (rediscretisation of the mean), 1 geometric, 2 harmonic */
   int autotune;           /* 1: time the stencil's x-chunk length per level at set-up */
+  int stencil_variant;    /* 0: chosen by the autotuner; else forced: 1 one voxel row per
+                             thread, 2 two rows per thread, 3 two load cases per thread in
+                             packed FP32x2 lanes, 4 two rows per thread in packed FP32x2
+                             lanes (3 and 4: FP32 operators; FP64 ones use 1 and 2) */
 } femh_config;
 
 typedef struct {
@@ -134,7 +138,9 @@ femh_status femh_fluctuation(femh_handle* h, double* chi_out, int out_on_device)
 
 /* Apply the periodic operator: y_I = K(rho) u_I for the 6 fields u, layout
  * [6][nx*ny*nz][3] (the reference's assembled K, e.g.
- * SamplesGenerator/NumericalCoarsening.cpp:1238-1306, matrix-free). */
+ * SamplesGenerator/NumericalCoarsening.cpp:1238-1306, matrix-free).  FP64
+ * unless the handle's precision is mixed with FP32 storage: then the FP32
+ * kernel the multigrid sweeps use (coefficients and u rounded to FP32). */
 femh_status femh_apply_operator(femh_handle* h, int nx, int ny, int nz, double hvox,
                                 const double* rho, const double* u, double* y, int on_device);
 

@@ -2,6 +2,8 @@
 
 Bars (written here):
   * operator apply, FP64:                 1e-13 relative (max-norm)
+  * operator apply, FP32 kernels:         2e-6 relative (max-norm; FP32 rounding
+                                          of rho-scaled coefficients, u and sums)
   * C^H, plain FP64 (Jacobi / GMG PCG):   1e-8 relative (max entry / max |C|)
   * C^H, mixed precision (FP32 inner):    1e-6 relative
   * gradients dL/drho, dC/drho:           1e-5 relative
@@ -14,6 +16,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 TOL_APPLY = 1e-13
+TOL_APPLY32 = 2e-6
 TOL_FP64 = 1e-8
 TOL_MIXED = 1e-6
 TOL_GRAD = 1e-5
@@ -37,6 +40,35 @@ def test_apply_matches_oracle(femh, oracle, rng, shape):
     mat = oracle.material()
     yo = oracle.apply(shape, oracle.k0(1.0, 0.3, 1.0 / shape[0]), oracle.coef(mat, rho), u)
     assert _rel(y, yo) < TOL_APPLY
+
+
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+@pytest.mark.parametrize("shape", [(16, 16, 16), (12, 8, 20), (8, 24, 24), (6, 10, 4), (8, 16, 128)])
+def test_fp32_stencil_variants_match_oracle(femh, oracle, rng, shape, variant):
+    """The FP32 kernels of the multigrid sweeps, each forced in turn: one voxel
+    row per thread, two rows per thread, two load cases per thread in packed
+    FP32x2 lanes, and two rows per thread in packed FP32x2 lanes
+    (compile-time and runtime z extents)."""
+    rho = 0.3 + 0.7 * rng.random(shape)
+    u = rng.standard_normal((6,) + shape + (3,))
+    e = femh.Engine(precision=femh.MIXED_PC, stencil_variant=variant, autotune=0)
+    y = e.apply_operator(rho, u)
+    mat = oracle.material()
+    yo = oracle.apply(shape, oracle.k0(1.0, 0.3, 1.0 / shape[0]), oracle.coef(mat, rho), u)
+    assert _rel(y, yo) < TOL_APPLY32
+
+
+@pytest.mark.parametrize("bf16", [0, 1])
+@pytest.mark.parametrize("shape", [(16, 16, 16), (16, 8, 24)])
+def test_mixed_pc_C_matches_oracle(femh, oracle, shape, bf16):
+    """FP64 CG with the FP32 multigrid preconditioner (the bench's mixed mode)."""
+    from fem_b200 import fields
+    rho = fields.smooth_cell(16, sigma=2.0, seed=3)[: shape[0], : shape[1], : shape[2]].copy()
+    Co, *_ = oracle.homogenize(rho)
+    e = femh.Engine(precision=femh.MIXED_PC, store_bf16=bf16)
+    C, info = e.homogenize(rho)
+    assert info["status"] == 0 and max(info["rel_residual"]) < 1e-10
+    assert _rel(C, Co) < TOL_MIXED
 
 
 def test_apply_deterministic(femh, rng):
