@@ -214,7 +214,8 @@ struct Level {
   int NT = 256, maxnz = 1;
   int nz_spec = 0;   // > 0: every cell of the level has this z extent (specialised kernel)
   int chunk = 0;     // x-chunk length of the stencil units (0 = heuristic), set by the autotuner
-  int variant = 2;   // stencil kernel: 2 = two voxel rows per thread, 1 = one row per thread
+  int variant = 2;   // stencil kernel (femh_config::stencil_variant numbering)
+  bool bulk_ok = false;   // the bulk-copy staged kernel (variant 5) can run on this level
   // level 0 of the mixed modes also runs FP64 operator applies (CG / true
   // residual): they get their own tuned layout (FP64 kernels spill in the
   // layout that suits FP32)
@@ -300,6 +301,7 @@ struct femh_handle {
   std::vector<double> C_last;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int* d_err = nullptr;   // set by a stencil kernel whose bounded wait ran out
 
   // measurement: per-kernel-class CUDA-event timing (femh_profile), and the
   // count of kernel executions including CUDA-graph replays
@@ -399,7 +401,7 @@ MatLaw make_law(const femh_config& c) {
 void add_stencil_units(std::vector<StencilUnit>& out, int cellidx, const CellDesc& cd, int NT,
                        int& slot, int chunk_req = 0, int variant = 2) {
   const int R = NT / cd.nz;
-  const bool two_rows = variant == 2 || variant == 4;
+  const bool two_rows = variant == 2 || variant == 4 || variant == 5;
   const int maxrows = std::max(1, std::min(two_rows ? 2 * R - 1 : R - 1, cd.ny));
   const int ntiles = (cd.ny + maxrows - 1) / maxrows;
   const int chunk = chunk_req > 0 ? std::min(chunk_req, cd.nx)
@@ -430,7 +432,7 @@ template <typename T> size_t esize() { return sizeof(T); }
 // needs up to ~160 registers a thread, so it runs 384-thread CTAs where its
 // tiles still hold at least two thread rows.
 int variant_nt(int level_nt, int maxnz, int variant) {
-  if (variant == 4 && level_nt > 384 && 384 >= 2 * maxnz) return 384;
+  if ((variant == 4 || variant == 5) && level_nt > 384 && 384 >= 2 * maxnz) return 384;
   return level_nt;
 }
 
@@ -487,6 +489,19 @@ void stencil_go4(femh_handle* H, dim3 grid, size_t smem, const StencilArgs<TIn, 
   LAUNCH_CHECK(H);
 }
 
+// Two voxel rows per thread in packed FP32x2 lanes, inputs staged by bulk copies (variant 5).
+template <int NT, int OUT, int NZ>
+void stencil_go5(femh_handle* H, dim3 grid, size_t smem, const StencilArgs<float, float, float, float>& a) {
+  static bool attr = false;
+  auto fn = stencil2b_kernel<NT, OUT, NZ>;
+  if (!attr) {   // (a few bytes of static shared memory come on top)
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr = true;
+  }
+  fn<<<grid, NT, smem, H->stream>>>(a);
+  LAUNCH_CHECK(H);
+}
+
 // T = arithmetic type; in/out/b storage types as given.
 template <typename T, int OUT, typename TIn, typename TOut, typename TB, typename TC>
 void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* out, const TB* b,
@@ -498,7 +513,14 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   int variant = use64 ? L.variant64 : L.variant;
   if (!std::is_same<T, float>::value) {   // packed-FP32 kernels: FP64 twin with the same units
     if (variant == 3) variant = 1;
-    if (variant == 4) variant = 2;
+    if (variant == 4 || variant == 5) variant = 2;
+  }
+  if (variant == 5) {   // bulk-copy staging: FP32 storage, 16-byte aligned rows, eligible level
+    const bool f32 = std::is_same<TIn, float>::value && std::is_same<TOut, float>::value &&
+                     std::is_same<TB, float>::value && std::is_same<TC, float>::value;
+    auto al = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+    if (!(f32 && L.bulk_ok && al(in) && al(out) && al(kc) && al(L.invd) && (!b || al(b)) && L.ntot % 4 == 0))
+      variant = 4;
   }
   StencilArgs<TIn, TOut, TB, TC> a;
   a.cells = L.d_cells;
@@ -513,6 +535,7 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   a.ntot = L.ntot;
   a.k = H->hk;
   a.omega = omega;
+  a.err = H->d_err;
   {
     const HadK& k = H->hk;
     const double kv[8] = {k.A, k.Bd - k.Bo, k.Bo, k.D1 - k.O1, k.O1, k.D2 - k.O2, k.O2, k.G};
@@ -544,6 +567,22 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   if (OUT >= OUT_JACOBI) per += 18.0 * sizeof(TB) + (OUT == OUT_RESID ? 0.0 : 4.0);
   std::string key(nm);
   Prof prof_(H, H->prof ? H->kstats.emplace(key, femh_handle::KStat{}).first->first.c_str() : nm, nodes * per);
+  if constexpr (std::is_same<TIn, float>::value && std::is_same<TOut, float>::value &&
+                std::is_same<TB, float>::value && std::is_same<TC, float>::value) {
+    if (variant == 5) {   // eligible levels have a compile-time z extent and 384-thread tiles
+      const int nt = variant_nt(L.NT, L.maxnz, 5);
+      const size_t sm5 = stencil2b_smem_bytes(nt, L.nz_spec);
+      switch (L.nz_spec) {
+        case 16: stencil_go5<384, OUT, 16>(H, grid, sm5, a); return;
+        case 24: stencil_go5<384, OUT, 24>(H, grid, sm5, a); return;
+        case 32: stencil_go5<384, OUT, 32>(H, grid, sm5, a); return;
+        case 48: stencil_go5<384, OUT, 48>(H, grid, sm5, a); return;
+        case 64: stencil_go5<384, OUT, 64>(H, grid, sm5, a); return;
+        case 128: stencil_go5<384, OUT, 128>(H, grid, sm5, a); return;
+        default: throw FemhError{FEMH_E_ARG, "bulk-copy stencil on an ineligible level"};
+      }
+    }
+  }
   if constexpr (std::is_same<T, float>::value) {
     if (variant == 4) {
       const int nt = variant_nt(L.NT, L.maxnz, 4);
@@ -695,7 +734,13 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
         L.NT = (z0 == 24 || z0 == 48) ? 480 : 512;
       }
     }
+    {   // bulk-copy staging needs 16-byte rows and at most two row segments per tile
+      L.bulk_ok = L.nz_spec > 0 && L.nz_spec % 4 == 0 && L.nz_spec <= 128;
+      const int tr = variant_nt(L.NT, L.maxnz, 5) / std::max(1, L.maxnz);
+      for (auto& cd : L.cells) L.bulk_ok = L.bulk_ok && cd.ny >= 2 * tr + 3;
+    }
     if (c.stencil_variant > 0) L.variant = c.stencil_variant;
+    if (L.variant == 5 && !L.bulk_ok) L.variant = 4;
     int ss = 0, sn = 0;
     for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
       const CellDesc& cd = L.cells[ci];
@@ -773,7 +818,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   const Level& L0 = H->levels[0];
   H->d_part_s = ar.arr<double>(std::max(L0.all.su.size(), L0.su64.size()) * kNumRhs);
   H->d_part_n = ar.arr<double>(L0.all.nu.size() * kNumRhs * 2);
-  H->d_part_z = ar.arr<double>(L0.all.nu.size() * kNumRhs);
+  H->d_part_z = ar.arr<double>(std::max(L0.all.nu.size(), L0.all.su.size()) * kNumRhs);
   H->d_part_e = ar.arr<double>(L0.all.nu.size() * 22);   // 21 pair energies + sum of rho per slot
   H->d_C = ar.arr<double>(nc * 36);
   H->d_W = ar.arr<double>(nc * 21);
@@ -972,6 +1017,7 @@ void autotune_levels(femh_handle* H, bool mg) {
       if (cand <= maxnx && std::find(cands.begin(), cands.end(), cand) == cands.end()) cands.push_back(cand);
     std::vector<int> vars = {1, 2};
     if (std::is_same<T, float>::value) vars = {2, 3, 4};
+    if (std::is_same<T, float>::value && L.bulk_ok) vars.push_back(5);
     if (H->cfg.stencil_variant > 0) vars = {H->cfg.stencil_variant};
     for (int var : vars)
     for (int cand : cands) {
@@ -1060,6 +1106,15 @@ void prepare_operator(femh_handle* H) {
 
 unsigned fin_blocks(int nc) { return cdiv((long long)nc * kNumRhs * 32, 128); }   // a warp per (cell, rhs)
 
+// The z . r product of the multigrid preconditioner comes out of the last
+// level-0 post-smoothing sweep when every level-0 cell is smoothed there (no
+// cell is solved directly on level 0) and there is such a sweep.
+bool fuse_rz(const femh_handle* H) {
+  const Level& L0 = H->levels[0];
+  return H->cfg.solver == FEMH_GMG_PCG && H->cfg.post_smooth > 0 && L0.coarse_list.empty() &&
+         L0.smooth.su.size() == L0.all.su.size();
+}
+
 // One V-cycle of the multigrid preconditioner: z = V(r0), levels in TM
 // arithmetic/storage with coefficients TMC; r0 (level-0 right-hand side) may
 // be of another type (FP64 CG residual feeding an FP32 V-cycle).  Level 0's xa
@@ -1100,7 +1155,7 @@ void vcycle_level_down(femh_handle* H, int l, const TB* b, TM* cur, TM* oth, TM*
 }
 
 template <typename TM, typename TMC, typename TB>
-void vcycle_level_up(femh_handle* H, int l, const TB* b, TM* x, TM* t, const TM* coarse_sol) {
+void vcycle_level_up(femh_handle* H, int l, const TB* b, TM* x, TM* t, const TM* coarse_sol, double* dot_part) {
   const femh_config& c = H->cfg;
   cudaStream_t s = H->stream;
   const CGState* stt = H->d_state;
@@ -1114,13 +1169,18 @@ void vcycle_level_up(femh_handle* H, int l, const TB* b, TM* x, TM* t, const TM*
     LAUNCH_CHECK(H);
   }
   for (int sw = 0; sw < c.post_smooth; ++sw) {
-    stencil<TM, OUT_JACOBI>(H, L, true, (const TM*)x, t, b, (const TMC*)L.kc, nullptr, stt, c.omega);
+    if (dot_part && sw + 1 == c.post_smooth)   // last sweep also forms z . b
+      stencil<TM, OUT_JACOBI_DOT>(H, L, true, (const TM*)x, t, b, (const TMC*)L.kc, dot_part, stt, c.omega);
+    else
+      stencil<TM, OUT_JACOBI>(H, L, true, (const TM*)x, t, b, (const TMC*)L.kc, nullptr, stt, c.omega);
     std::swap(x, t);
   }
 }
 
+// dot_part != nullptr: the last level-0 sweep writes the z . r0 partials
+// there (per stencil unit slot).
 template <typename TM, typename TMC, typename TR>
-TM* vcycle(femh_handle* H, const TR* r0) {
+TM* vcycle(femh_handle* H, const TR* r0, double* dot_part) {
   const femh_config& c = H->cfg;
   const int nlev = (int)H->levels.size();
   std::vector<TM*> sm(nlev), tmp(nlev), sol(nlev);
@@ -1139,8 +1199,8 @@ TM* vcycle(femh_handle* H, const TR* r0) {
                                          (TM*)H->levels[l].xb, sol[l]);
   }
   for (int l = nlev - 2; l >= 0; --l) {
-    if (l == 0) vcycle_level_up<TM, TMC, TR>(H, 0, r0, sm[0], tmp[0], sol[1]);
-    else vcycle_level_up<TM, TMC, TM>(H, l, (const TM*)H->levels[l].bv, sm[l], tmp[l], sol[l + 1]);
+    if (l == 0) vcycle_level_up<TM, TMC, TR>(H, 0, r0, sm[0], tmp[0], sol[1], dot_part);
+    else vcycle_level_up<TM, TMC, TM>(H, l, (const TM*)H->levels[l].bv, sm[l], tmp[l], sol[l + 1], nullptr);
   }
   return sol[0];
 }
@@ -1190,15 +1250,20 @@ void pcg_iteration(femh_handle* H, const typename PR::K* kcg) {
     LAUNCH_CHECK(H);
   }
   TM* z = nullptr;
+  const bool fuse = fuse_rz(H);
   if (gmg) {
-    z = rm ? vcycle<TM, TMC, TM>(H, rm) : vcycle<TM, TMC, TV>(H, r);
-    Prof prof_(H, "k_dot", 0.0);
-    k_dot<TM, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
-    LAUNCH_CHECK(H);
+    double* dp = fuse ? H->d_part_z : nullptr;
+    z = rm ? vcycle<TM, TMC, TM>(H, rm, dp) : vcycle<TM, TMC, TV>(H, r, dp);
+    if (!fuse) {
+      Prof prof_(H, "k_dot", 0.0);
+      k_dot<TM, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
+      LAUNCH_CHECK(H);
+    }
   }
   {
     Prof prof_(H, "k_fin_beta", 0.0);
-    k_fin_beta<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_n, H->d_part_z, nc,
+    k_fin_beta<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, fuse ? L0.d_su_sb : L0.d_nu_sb,
+                                              fuse ? L0.d_su_se : L0.d_nu_se, H->d_part_n, H->d_part_z, nc,
                                               gmg ? 0 : 1);
     LAUNCH_CHECK(H);
   }
@@ -1251,15 +1316,18 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
                                                           L0.invd, c.omega, stt, L0.ntot);
       LAUNCH_CHECK(H);
     }
-    TM* z = rm ? vcycle<TM, TMC, TM>(H, rm) : vcycle<TM, TMC, TV>(H, r);
-    {
+    const bool fuse = fuse_rz(H);
+    double* dp = fuse ? H->d_part_z : nullptr;
+    TM* z = rm ? vcycle<TM, TMC, TM>(H, rm, dp) : vcycle<TM, TMC, TV>(H, r, dp);
+    if (!fuse) {
       Prof prof_(H, "k_dot", 0.0);
       k_dot<TM, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, z, r, stt, H->d_part_z, L0.ntot);
       LAUNCH_CHECK(H);
     }
     {
       Prof prof_(H, "k_fin_rz", 0.0);
-      k_fin_rz<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_z, H->d_part_n, nc);
+      k_fin_rz<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, fuse ? L0.d_su_sb : L0.d_nu_sb,
+                                              fuse ? L0.d_su_se : L0.d_nu_se, H->d_part_z, H->d_part_n, nc);
       LAUNCH_CHECK(H);
     }
     {   // p = z (beta = 0; Jacobi z for pairs that fell back)
@@ -1521,6 +1589,18 @@ void energy_C(femh_handle* H, std::vector<double>& C, std::vector<double>& dens)
 }
 
 // Common path of single-cell and batched calls.  rho_ptrs[i] host or device.
+// A kernel whose bounded wait ran out leaves its work undone and sets the
+// handle's error flag: report it (and clear it) at the end of a solve.
+void check_kernel_error(femh_handle* H) {
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, H->d_err, sizeof(int), cudaMemcpyDeviceToHost, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  if (e) {
+    CK(cudaMemsetAsync(H->d_err, 0, sizeof(int), H->stream));
+    throw FemhError{FEMH_E_CUDA, "a stencil kernel's copy pipeline timed out"};
+  }
+}
+
 void run_cells(femh_handle* H, const std::vector<int>& shapes, const std::vector<double>& hs,
                const std::vector<const double*>& rho, bool rho_dev, std::vector<double>& C,
                std::vector<femh_solve_info>& infos) {
@@ -1532,6 +1612,7 @@ void run_cells(femh_handle* H, const std::vector<int>& shapes, const std::vector
                        rho_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
   }
   solve_all(H, infos);
+  check_kernel_error(H);
   std::vector<double> dens;
   energy_C(H, C, dens);
   for (int i = 0; i < H->ncells; ++i) infos[i].density = dens[i];
@@ -1638,6 +1719,8 @@ femh_status femh_create(femh_handle** out, const femh_config* cfg) {
     H->d_K0 = H->perm.arr<double>(576);
     CK(cudaMemcpy(H->d_ec, &H->ec, sizeof(ElemConst), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(H->d_K0, H->K0, sizeof(double) * 576, cudaMemcpyHostToDevice));
+    H->d_err = H->perm.arr<int>(1);
+    CK(cudaMemset(H->d_err, 0, sizeof(int)));
   });
   if (st != FEMH_OK) {
     femh_destroy(H);
@@ -1872,6 +1955,7 @@ femh_status femh_apply_operator(femh_handle* H, int nx, int ny, int nz, double h
       LAUNCH_CHECK(H);
       stencil<float, OUT_APPLY>(H, L0, false, (const float*)uf, yf, (const float*)nullptr, (const float*)L0.kc,
                                 nullptr, nullptr, 0.0);
+      check_kernel_error(H);
       k_copy<double, float><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->b64, yf, nullptr,
                                                               L0.ntot);
       LAUNCH_CHECK(H);

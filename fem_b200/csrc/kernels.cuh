@@ -293,12 +293,15 @@ __global__ void k_fin_init(CGState* stt, const int* slot_begin, const int* slot_
 // rz for the multigrid preconditioner at start (z . r of the first V-cycle);
 // if that is not positive, the pair starts with the Jacobi preconditioner.
 // beta = 0 so that the following direction kernel sets p = z.
+// part: z.r partials over slot range [zb, ze) of each cell (node units, or the
+// stencil units of the sweep that computed them); part_init: the start
+// partials over [slot_begin, slot_end).
 __global__ void k_fin_rz(CGState* stt, const int* slot_begin, const int* slot_end,
-                         const double* part, const double* part_init, int ncells) {
+                         const int* zb, const int* ze, const double* part, const double* part_init, int ncells) {
   FIN_PROLOGUE
   CGState S = stt[t];
   if (!S.active) return;
-  const double rz_mg = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 1, 0);
+  const double rz_mg = sum_slots(part, zb[cell], ze[cell], rhs, 1, 0);
   const double rz_jac = sum_slots(part_init, slot_begin[cell], slot_end[cell], rhs, 2, 1);
   S.beta = 0.0;
   if (isfinite(rz_mg) && rz_mg > 0.0) {
@@ -330,15 +333,17 @@ __global__ void k_fin_alpha(CGState* stt, const int* slot_begin, const int* slot
 
 // After the update (+ preconditioner): convergence test and beta.
 // jacobi: rz_new from the update partials; else from the V-cycle partials.
+// part_rz: z.r partials over slot range [zb, ze) of each cell.
 __global__ void k_fin_beta(CGState* stt, const int* slot_begin, const int* slot_end,
-                           const double* part_upd, const double* part_rz, int ncells, int jacobi) {
+                           const int* zb, const int* ze, const double* part_upd, const double* part_rz,
+                           int ncells, int jacobi) {
   FIN_PROLOGUE
   CGState S = stt[t];
   if (!S.active) return;
   const int b = slot_begin[cell], e = slot_end[cell];
   const double rr = sum_slots(part_upd, b, e, rhs, 2, 0);
   const double rz_jac = sum_slots(part_upd, b, e, rhs, 2, 1);
-  const double rz_mg = jacobi ? rz_jac : sum_slots(part_rz, b, e, rhs, 1, 0);
+  const double rz_mg = jacobi ? rz_jac : sum_slots(part_rz, zb[cell], ze[cell], rhs, 1, 0);
   const double rzn = (jacobi || S.fallback) ? rz_jac : rz_mg;
   S.rr = rr;
   S.iters += 1;

@@ -49,6 +49,7 @@ struct StencilArgs {
   HadK k;
   double omega;
   float2 kp[8];          // FP32 pairs (x = y) of A, Bd-Bo, Bo, D1-O1, O1, D2-O2, O2, G
+  int* err;              // set non-zero by a kernel whose bounded wait ran out
 };
 
 template <typename T>
@@ -1207,6 +1208,349 @@ stencil2p_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
     block_reduce<1>(v, red);
     if (tid == 0) a.partials[(long long)un.slot * kNumRhs + rhs] = v[0];
   }
+}
+
+// ------------------------------------------------ bulk-copy staging ---
+// mbarrier + cp.async.bulk helpers (PTX; addresses are shared-window offsets).
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for a phase of an mbarrier: false if it did not complete
+// within the iteration limit (each try_wait also suspends for a while).
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  for (int it = 0; it < (1 << 20); ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// stencil2p_kernel with its inputs staged by bulk copies (FP32 storage).  A
+// stage holds, for step s (voxel plane ie = i0-1+s), node plane ie+1 of u
+// (node rows j0-1 .. j0+rows+1), voxel plane ie of kc (voxel rows j0-1 ..
+// j0+rows) and, for the gather of node plane ie-1, b and invd of the owned
+// node rows j0 .. j0+rows-1.  Rows of the z ring are contiguous in memory, so
+// a stage is a handful of row-segment copies (split where y wraps) that the
+// lanes of warp 0 issue against one mbarrier.  A ring of kBulkSlots stages
+// runs kBulkSlots-1 steps ahead of the one in use; no per-thread loads of
+// inputs remain.
+// Requirements (checked by the host): nz % 4 == 0 on every cell, 16-byte
+// aligned arrays, ny >= 2*TR+3 so that each array needs at most two segments.
+constexpr int kBulkSlots = 4;
+
+template <int NT, int OUT, int NZ>
+__global__ void __launch_bounds__(NT, 1)
+stencil2b_kernel(StencilArgs<float, float, float, float> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const StencilUnit un = a.units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cd = a.cells[un.cell];
+  if (a.stt && !a.stt[cd.id * kNumRhs + rhs].active) return;
+  const int nx = cd.nx, ny = cd.ny;
+  const int nz = NZ > 0 ? NZ : cd.nz;
+  const int TR = NT / nz;
+  const int tid = threadIdx.x;
+  const int t = tid / nz, z = tid - t * nz;
+  const int rows = un.rows;
+  const bool live = t < TR && 2 * t <= rows;
+  const bool own1 = live && 2 * t < rows;
+  const bool own2 = live && 2 * t + 1 < rows;
+  const int zp = (z + 1 == nz) ? 0 : z + 1;
+  const int zm = (z == 0) ? nz - 1 : z - 1;
+  auto wrapy = [&](int j) { j %= ny; return j < 0 ? j + ny : j; };
+  const int n1 = wrapy(un.j0 + 2 * t), n2 = wrapy(un.j0 + 2 * t + 1);
+
+  // stage layout (floats): U[3][NRU][nz], KC[NRK][nz], B[3][rows][nz], ID[rows][nz]
+  const int NRU = rows + 3, NRK = rows + 2;
+  const int oK = 3 * NRU * nz, oB = oK + NRK * nz, oI = oB + 3 * rows * nz;
+  const int SS = (oI + rows * nz + 3) & ~3;   // floats per stage, 16-byte multiple
+  const int PS = TR * 3 * nz;
+  float* stg = reinterpret_cast<float*>(smem_raw);
+  f2* QAB = reinterpret_cast<f2*>(stg + kBulkSlots * SS);   // [2][TR][3][nz]
+  f2* QCD = QAB + 2 * PS;
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(QCD + 2 * PS);
+  double* red = reinterpret_cast<double*>(bars + kBulkSlots);
+  __shared__ int abort_flag;
+  const int pt = t * 3 * nz;
+  const int pa = (t + 1 < TR ? t + 1 : t) * 3 * nz;
+
+  const long long st = a.ntot;
+  const int plane = ny * nz;
+  const int c1 = n1 * nz + z, c2 = n2 * nz + z;
+  float* obase = a.out + (long long)rhs * 3 * st + cd.off;
+
+  // copy descriptors: lane l of warp 0 owns copy l (at most 16 are used)
+  const char* src_base = nullptr;   // array base for this lane's copy (cell offset included)
+  int plane_lag = 0, src_off = 0, dst_off = 0, bytes = 0;
+  unsigned tx_total = 0;
+  if (tid < 32) {
+    int idx = 0;
+    auto seg = [&](const float* base, int lag, int row0, int nrows, int dst) {
+      int done = 0;
+      while (done < nrows) {
+        const int r0 = wrapy(row0 + done);
+        const int n = min(nrows - done, ny - r0);
+        if (idx == tid) {
+          src_base = reinterpret_cast<const char*>(base);
+          plane_lag = lag;
+          src_off = r0 * nz;
+          dst_off = dst + done * nz;
+          bytes = n * nz * 4;
+        }
+        tx_total += (unsigned)(n * nz * 4);
+        ++idx;
+        done += n;
+      }
+    };
+    for (int c = 0; c < 3; ++c) seg(a.u + ((long long)rhs * 3 + c) * st + cd.off, 1, un.j0 - 1, NRU, c * NRU * nz);
+    seg(a.kc + cd.off, 0, un.j0 - 1, NRK, oK);
+    if (OUT >= OUT_JACOBI) {
+      for (int c = 0; c < 3; ++c)
+        seg(a.b + ((long long)rhs * 3 + c) * st + cd.off, -1, un.j0, rows, oB + c * rows * nz);
+      if (OUT != OUT_RESID) seg(a.invd + cd.off, -1, un.j0, rows, oI);
+    }
+  }
+  // stage g (= step g-1) is node plane i0-2+g of u, voxel plane i0-2+g of kc
+  // and node plane i0-3+g of b / invd; lag = plane offset relative to i0-2+g.
+  int issued = 0;   // stages issued so far (warp 0)
+  auto issue = [&](int g) {
+    issued = g + 1;
+    const int slot = g % kBulkSlots;
+    const unsigned bar = smem_addr(bars + slot);
+    if (tid == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(bar, tx_total);
+    }
+    __syncwarp();
+    if (bytes > 0) {
+      int pl = (un.i0 - 2 + g + plane_lag) % nx;
+      if (pl < 0) pl += nx;
+      bulk_g2s(smem_addr(stg + slot * SS + dst_off), src_base + 4LL * ((long long)pl * plane + src_off),
+               (unsigned)bytes, bar);
+    }
+  };
+  const int G = un.len + 3;   // stages 0 .. len+2 (step -1 .. len+1)
+  if (tid == 0) {
+    for (int k = 0; k < kBulkSlots; ++k) mbar_init(smem_addr(bars + k), 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid < 32)
+    for (int g = 0; g < kBulkSlots && g < G; ++g) issue(g);
+  int waited = 0;   // stages this thread has waited for (for the exit drain)
+  auto wait_stage = [&](int g) {
+    if (!mbar_wait(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1))) {
+      if (a.err) atomicExch(a.err, 1);
+      abort_flag = 1;
+    }
+    waited = g + 1;
+  };
+
+  f2 prv[3][4], car[3][4];
+  f2 own[3], u12[3], raw[3];
+  int pg = 0;
+  double acc = 0.0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) own[c] = u12[c] = raw[c] = p_bc(0.f);
+
+  auto patch = [&](const float* U, f2 (&h)[3][4], f2 (&mine)[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float* Uc = U + c * NRU * nz;
+      const int r0 = (2 * t) * nz;
+      mine[c] = make_float2(Uc[r0 + nz + z], Uc[r0 + 2 * nz + z]);
+      const f2 up = make_float2(Uc[r0 + nz + zp], Uc[r0 + 2 * nz + zp]);
+      h[c][0] = make_float2(Uc[r0 + z], mine[c].x);
+      h[c][1] = make_float2(Uc[r0 + zp], up.x);
+      h[c][2] = mine[c];
+      h[c][3] = up;
+      had4_fwd(h[c]);
+    }
+  };
+  auto gather = [&](int buf, const float* S) {
+    const f2* Qab = QAB + buf * PS;
+    const f2* Qcd = QCD + buf * PS;
+    f2 y[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      y[c] = p_add(own[c], Qab[pt + c * nz + zm]);
+      y[c].y += Qcd[pa + c * nz + z].x + Qcd[pa + c * nz + zm].y;
+    }
+    float* ob = obase + pg;
+    const int r1 = (2 * t) * nz + z, r2 = r1 + nz;   // owned rows in the b / invd arrays
+    if (OUT == OUT_APPLY || OUT == OUT_APPLY_DOT) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (own1) ob[c * st + c1] = y[c].x;
+        if (own2) ob[c * st + c2] = y[c].y;
+        if (OUT == OUT_APPLY_DOT) {
+          if (own1) acc += (double)u12[c].x * (double)y[c].x;
+          if (own2) acc += (double)u12[c].y * (double)y[c].y;
+        }
+      }
+    } else {
+      const bool pin1 = (pg + c1 == 0), pin2 = (pg + c2 == 0);
+      const float* Bs = S + oB;
+      f2 wd = p_bc(0.f);
+      if (OUT != OUT_RESID) {
+        const float* Is = S + oI;
+        wd = p_mul(p_bc((float)a.omega), make_float2(own1 ? Is[r1] : 0.f, own2 ? Is[r2] : 0.f));
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const f2 bv = make_float2(own1 ? Bs[c * rows * nz + r1] : 0.f, own2 ? Bs[c * rows * nz + r2] : 0.f);
+        const f2 d = p_sub(bv, y[c]);
+        if (OUT == OUT_RESID) {
+          if (own1) ob[c * st + c1] = pin1 ? 0.f : d.x;
+          if (own2) ob[c * st + c2] = pin2 ? 0.f : d.y;
+        } else {
+          const f2 xv = p_fma(wd, d, u12[c]);
+          if (own1) ob[c * st + c1] = xv.x;
+          if (own2) ob[c * st + c2] = xv.y;
+          if (OUT == OUT_JACOBI_DOT) {
+            if (own1) acc += (double)xv.x * (double)bv.x;
+            if (own2) acc += (double)xv.y * (double)bv.y;
+          }
+        }
+      }
+    }
+  };
+
+  // step -1 (stage 0): transformed patches of node plane i0-1
+  wait_stage(0);
+  if (live) {
+    f2 mine[3];
+    patch(stg, prv, mine);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      raw[c] = mine[c];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) car[c][q] = p_bc(0.f);
+    }
+  }
+  for (int s = 0; s <= un.len + 1; ++s) {
+    const int g = s + 1;
+    wait_stage(g);
+    __syncthreads();   // stage g complete for all; Q[(s-1)&1] complete; slot of stage g-1 free
+    if (abort_flag) break;
+    if (tid < 32 && g + kBulkSlots - 1 < G) issue(g + kBulkSlots - 1);   // the slot of stage g-1
+    const float* S = stg + (g % kBulkSlots) * SS;
+    const int pe = ((un.i0 - 1 + s + nx) % nx) * plane;   // voxel plane ie
+    if (s >= 2 && live) gather((s - 1) & 1, S);
+    if (s > un.len || !live) continue;
+    f2 w[3][8];
+    f2 cur0[3];
+    {
+      f2 cur[3][4];
+      patch(S, cur, cur0);
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (q > 0) w[c][q] = p_add(cur[c][q], prv[c][q]);
+          w[c][4 + q] = p_sub(cur[c][q], prv[c][q]);
+          prv[c][q] = cur[c][q];
+        }
+    }
+    {
+      const float* K = S + oK + (2 * t) * nz + z;
+      const f2 kv = make_float2(K[0], K[nz]);
+      const f2 A = p_mul(kv, a.kp[0]), Bdo = p_mul(kv, a.kp[1]), Bo = p_mul(kv, a.kp[2]);
+      const f2 D1o = p_mul(kv, a.kp[3]), O1 = p_mul(kv, a.kp[4]);
+      const f2 D2o = p_mul(kv, a.kp[5]), O2 = p_mul(kv, a.kp[6]), Gd = p_mul(kv, a.kp[7]);
+      {
+        const f2 m0 = w[0][4], m1 = w[1][2], m2 = w[2][1];
+        const f2 tt = p_mul(Bo, p_add(p_add(m0, m1), m2));
+        w[0][4] = p_fma(Bdo, m0, tt); w[1][2] = p_fma(Bdo, m1, tt); w[2][1] = p_fma(Bdo, m2, tt);
+      }
+      {
+        const f2 sxz = p_mul(A, p_add(w[0][1], w[2][4]));
+        const f2 syz = p_mul(A, p_add(w[1][1], w[2][2]));
+        const f2 sxy = p_mul(A, p_add(w[0][2], w[1][4]));
+        w[0][1] = sxz; w[2][4] = sxz; w[1][1] = syz; w[2][2] = syz; w[0][2] = sxy; w[1][4] = sxy;
+      }
+      {
+        const f2 m0 = w[0][3], m1 = w[1][5], m2 = w[2][6];
+        const f2 tt = p_mul(O1, p_add(p_add(m0, m1), m2));
+        w[0][3] = p_fma(D1o, m0, tt); w[1][5] = p_fma(D1o, m1, tt); w[2][6] = p_fma(D1o, m2, tt);
+      }
+      {
+        const f2 x0 = w[1][3], x1 = w[0][5], tt = p_mul(O2, p_add(x0, x1));
+        w[1][3] = p_fma(D2o, x0, tt); w[0][5] = p_fma(D2o, x1, tt);
+      }
+      {
+        const f2 x0 = w[2][3], x1 = w[0][6], tt = p_mul(O2, p_add(x0, x1));
+        w[2][3] = p_fma(D2o, x0, tt); w[0][6] = p_fma(D2o, x1, tt);
+      }
+      {
+        const f2 x0 = w[2][5], x1 = w[1][6], tt = p_mul(O2, p_add(x0, x1));
+        w[2][5] = p_fma(D2o, x0, tt); w[1][6] = p_fma(D2o, x1, tt);
+      }
+      w[0][7] = p_mul(w[0][7], Gd); w[1][7] = p_mul(w[1][7], Gd); w[2][7] = p_mul(w[2][7], Gd);
+    }
+    f2* Qab = QAB + (s & 1) * PS;
+    f2* Qcd = QCD + (s & 1) * PS;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      f2 tot[4];
+      tot[0] = p_sub(car[c][0], w[c][4]);
+      car[c][0] = w[c][4];
+#pragma unroll
+      for (int q = 1; q < 4; ++q) {
+        tot[q] = p_add(p_sub(w[c][q], w[c][4 + q]), car[c][q]);
+        car[c][q] = p_add(w[c][q], w[c][4 + q]);
+      }
+      had4_inv(tot);
+      own[c] = make_float2(tot[0].y + tot[2].x, tot[2].y);
+      u12[c] = raw[c];
+      raw[c] = cur0[c];
+      if (s > 0) {
+        Qab[pt + c * nz + z] = make_float2(tot[1].y + tot[3].x, tot[3].y);
+        Qcd[pt + c * nz + z] = make_float2(tot[0].x, tot[1].x);
+      }
+    }
+    pg = pe;
+  }
+  // drain: every issued stage completes before the CTA's shared memory goes
+  // (bounded; only reached with stages outstanding after an abort)
+  if (tid == 0) {
+    for (int g = waited; g < issued; ++g)
+      if (!mbar_wait(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1))) break;
+  }
+  if (OUT == OUT_APPLY_DOT || OUT == OUT_JACOBI_DOT) {
+    double v[1] = {acc};
+    block_reduce<1>(v, red);
+    if (tid == 0) a.partials[(long long)un.slot * kNumRhs + rhs] = v[0];
+  }
+}
+
+// Shared memory bytes of one stencil2b_kernel CTA (tiles of up to 2*TR-1 rows).
+inline size_t stencil2b_smem_bytes(int NT, int nz) {
+  const int TR = NT / nz, rows = 2 * TR - 1;
+  const size_t SS = ((size_t)(3 * (rows + 3) + (rows + 2) + 4 * rows) * nz + 3) & ~(size_t)3;
+  return sizeof(float) * kBulkSlots * SS + sizeof(f2) * 4 * (size_t)TR * 3 * nz +
+         sizeof(unsigned long long) * kBulkSlots + 64 * sizeof(double);
 }
 
 // Shared memory bytes of one stencil2p_kernel CTA.

@@ -42,16 +42,19 @@ def test_apply_matches_oracle(femh, oracle, rng, shape):
     assert _rel(y, yo) < TOL_APPLY
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4])
-@pytest.mark.parametrize("shape", [(16, 16, 16), (12, 8, 20), (8, 24, 24), (6, 10, 4), (8, 16, 128)])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("shape", [(16, 16, 16), (12, 8, 20), (8, 24, 24), (6, 10, 4), (8, 16, 128),
+                                   (6, 20, 64), (4, 32, 32), (5, 11, 128)])
 def test_fp32_stencil_variants_match_oracle(femh, oracle, rng, shape, variant):
     """The FP32 kernels of the multigrid sweeps, each forced in turn: one voxel
     row per thread, two rows per thread, two load cases per thread in packed
-    FP32x2 lanes, and two rows per thread in packed FP32x2 lanes
-    (compile-time and runtime z extents)."""
+    FP32x2 lanes, two rows per thread in packed FP32x2 lanes, and the same with
+    its inputs staged by bulk copies (compile-time and runtime z extents; the
+    last three shapes meet the staged kernel's row condition, the others run
+    its fallback)."""
     rho = 0.3 + 0.7 * rng.random(shape)
     u = rng.standard_normal((6,) + shape + (3,))
-    e = femh.Engine(precision=femh.MIXED_PC, stencil_variant=variant, autotune=0)
+    e = femh.Engine(precision=femh.MIXED_PC, solver=femh.JACOBI_PCG, stencil_variant=variant, autotune=0)
     y = e.apply_operator(rho, u)
     mat = oracle.material()
     yo = oracle.apply(shape, oracle.k0(1.0, 0.3, 1.0 / shape[0]), oracle.coef(mat, rho), u)
