@@ -215,7 +215,8 @@ struct Level {
   int nz_spec = 0;   // > 0: every cell of the level has this z extent (specialised kernel)
   int chunk = 0;     // x-chunk length of the stencil units (0 = heuristic), set by the autotuner
   int variant = 2;   // stencil kernel (femh_config::stencil_variant numbering)
-  bool bulk_ok = false;   // the bulk-copy staged kernel (variant 5) can run on this level
+  bool bulk_ok = false;     // the bulk-copy staged FP32 kernel (variant 5) can run on this level
+  bool bulk_ok64 = false;   // the bulk-copy staged FP64 kernel (variant 6) can run on this level
   // level 0 of the mixed modes also runs FP64 operator applies (CG / true
   // residual): they get their own tuned layout (FP64 kernels spill in the
   // layout that suits FP32)
@@ -502,6 +503,19 @@ void stencil_go5(femh_handle* H, dim3 grid, size_t smem, const StencilArgs<float
   LAUNCH_CHECK(H);
 }
 
+// FP64 operator, one voxel row per thread, inputs staged by bulk copies (variant 6).
+template <int NT, int OUT, int NZ, typename TIn>
+void stencil_go6(femh_handle* H, dim3 grid, size_t smem, const StencilArgs<TIn, double, double, double>& a) {
+  static bool attr = false;
+  auto fn = stencil1b_kernel<NT, OUT, NZ, TIn>;
+  if (!attr) {   // (a few bytes of static shared memory come on top)
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    attr = true;
+  }
+  fn<<<grid, NT, smem, H->stream>>>(a);
+  LAUNCH_CHECK(H);
+}
+
 // T = arithmetic type; in/out/b storage types as given.
 template <typename T, int OUT, typename TIn, typename TOut, typename TB, typename TC>
 void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* out, const TB* b,
@@ -514,6 +528,16 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   if (!std::is_same<T, float>::value) {   // packed-FP32 kernels: FP64 twin with the same units
     if (variant == 3) variant = 1;
     if (variant == 4 || variant == 5) variant = 2;
+  } else if (variant == 6) {   // the staged FP64 kernel's FP32 twin has the same units
+    variant = 1;
+  }
+  if (variant == 6) {   // bulk-copy staging: FP64 output / rhs / coefficients, aligned rows
+    const bool ok = std::is_same<TOut, double>::value && std::is_same<TB, double>::value &&
+                    std::is_same<TC, double>::value &&
+                    (std::is_same<TIn, double>::value || std::is_same<TIn, float>::value);
+    auto al = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+    if (!(ok && L.bulk_ok64 && al(in) && al(out) && al(kc) && al(L.invd) && (!b || al(b)) && L.ntot % 4 == 0))
+      variant = 1;
   }
   if (variant == 5) {   // bulk-copy staging: FP32 storage, 16-byte aligned rows, eligible level
     const bool f32 = std::is_same<TIn, float>::value && std::is_same<TOut, float>::value &&
@@ -567,6 +591,23 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   if (OUT >= OUT_JACOBI) per += 18.0 * sizeof(TB) + (OUT == OUT_RESID ? 0.0 : 4.0);
   std::string key(nm);
   Prof prof_(H, H->prof ? H->kstats.emplace(key, femh_handle::KStat{}).first->first.c_str() : nm, nodes * per);
+  if constexpr (std::is_same<T, double>::value && std::is_same<TOut, double>::value &&
+                std::is_same<TB, double>::value && std::is_same<TC, double>::value &&
+                (std::is_same<TIn, double>::value || std::is_same<TIn, float>::value)) {
+    if (variant == 6) {
+      const size_t sm6 = stencil1b_smem_bytes(L.NT, L.nz_spec, (int)sizeof(TIn));
+      switch (L.nz_spec) {
+        case 16: stencil_go6<512, OUT, 16>(H, grid, sm6, a); return;
+        case 24: stencil_go6<480, OUT, 24>(H, grid, sm6, a); return;
+        case 32: stencil_go6<512, OUT, 32>(H, grid, sm6, a); return;
+        case 48: stencil_go6<480, OUT, 48>(H, grid, sm6, a); return;
+        case 64: stencil_go6<512, OUT, 64>(H, grid, sm6, a); return;
+        case 128: stencil_go6<512, OUT, 128>(H, grid, sm6, a); return;
+        case 256: stencil_go6<512, OUT, 256>(H, grid, sm6, a); return;
+        default: throw FemhError{FEMH_E_ARG, "staged FP64 stencil on an ineligible level"};
+      }
+    }
+  }
   if constexpr (std::is_same<TIn, float>::value && std::is_same<TOut, float>::value &&
                 std::is_same<TB, float>::value && std::is_same<TC, float>::value) {
     if (variant == 5) {   // eligible levels have a compile-time z extent and 384-thread tiles
@@ -738,6 +779,11 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
       L.bulk_ok = L.nz_spec > 0 && L.nz_spec % 4 == 0 && L.nz_spec <= 128;
       const int tr = variant_nt(L.NT, L.maxnz, 5) / std::max(1, L.maxnz);
       for (auto& cd : L.cells) L.bulk_ok = L.bulk_ok && cd.ny >= 2 * tr + 3;
+    }
+    {
+      L.bulk_ok64 = L.nz_spec > 0 && L.nz_spec % 4 == 0;
+      const int r64 = L.NT / std::max(1, L.maxnz);
+      for (auto& cd : L.cells) L.bulk_ok64 = L.bulk_ok64 && cd.ny >= r64 + 2;
     }
     if (c.stencil_variant > 0) L.variant = c.stencil_variant;
     if (L.variant == 5 && !L.bulk_ok) L.variant = 4;
@@ -927,7 +973,7 @@ void build_stencil_units64(femh_handle* H, Level& L, int chunk, int variant) {
 void autotune_level0_fp64(femh_handle* H) {
   Level& L = H->levels[0];
   cudaStream_t s = H->stream;
-  std::string key = "f64L0:" + std::to_string(L.NT);
+  std::string key = "f64L0:" + std::to_string(L.NT) + ":" + std::to_string(H->cfg.stencil_variant);
   int maxnx = 1;
   for (auto& cd : L.cells) {
     key += ":" + std::to_string(cd.nx) + "x" + std::to_string(cd.ny) + "x" + std::to_string(cd.nz);
@@ -935,12 +981,12 @@ void autotune_level0_fp64(femh_handle* H) {
   }
   auto it = H->tune_cache.find(key);
   if (it != H->tune_cache.end()) {
-    build_stencil_units64(H, L, it->second / 4, it->second % 4);
+    build_stencil_units64(H, L, it->second / 16, it->second % 16);
     return;
   }
   if (!H->cfg.autotune || L.ntot < 4096) {
     build_stencil_units64(H, L, 0, 1);
-    H->tune_cache[key] = 0 * 4 + 1;
+    H->tune_cache[key] = 0 * 16 + 1;
     return;
   }
   double* in = H->x64;
@@ -952,7 +998,10 @@ void autotune_level0_fp64(femh_handle* H) {
   std::vector<int> cands;
   for (int cand : {4, 8, 16, 32, 64, maxnx})
     if (cand <= maxnx && std::find(cands.begin(), cands.end(), cand) == cands.end()) cands.push_back(cand);
-  for (int var : {1, 2})
+  std::vector<int> vars64 = {1, 2};
+  if (L.bulk_ok64) vars64.push_back(6);
+  if (H->cfg.stencil_variant == 6 && L.bulk_ok64) vars64 = {6};
+  for (int var : vars64)
     for (int cand : cands) {
       build_stencil_units64(H, L, cand, var);
       float ms_min = 1e30f;
@@ -974,7 +1023,7 @@ void autotune_level0_fp64(femh_handle* H) {
       }
     }
   build_stencil_units64(H, L, best, best_var);
-  H->tune_cache[key] = best * 4 + best_var;
+  H->tune_cache[key] = best * 16 + best_var;
 }
 
 // Project autotuner for the stencil's tile shape: for every level whose
@@ -996,13 +1045,13 @@ void autotune_levels(femh_handle* H, bool mg) {
       maxnx = std::max(maxnx, cd.nx);
     }
     auto it = H->tune_cache.find(key);
-    if (it != H->tune_cache.end()) {   // cached: chunk * 4 + variant
-      L.variant = it->second % 4;
-      build_stencil_units(H, L, it->second / 4);
+    if (it != H->tune_cache.end()) {   // cached: chunk * 16 + variant
+      L.variant = it->second % 16;
+      build_stencil_units(H, L, it->second / 16);
       continue;
     }
     if (L.ntot < 4096) {   // tiny levels: launch-bound, the heuristic is fine
-      H->tune_cache[key] = L.chunk * 4 + L.variant;
+      H->tune_cache[key] = L.chunk * 16 + L.variant;
       continue;
     }
     T* in = (T*)(L.xa ? L.xa : H->cg_r);
@@ -1018,6 +1067,7 @@ void autotune_levels(femh_handle* H, bool mg) {
     std::vector<int> vars = {1, 2};
     if (std::is_same<T, float>::value) vars = {2, 3, 4};
     if (std::is_same<T, float>::value && L.bulk_ok) vars.push_back(5);
+    if (std::is_same<T, double>::value && L.bulk_ok64) vars.push_back(6);
     if (H->cfg.stencil_variant > 0) vars = {H->cfg.stencil_variant};
     for (int var : vars)
     for (int cand : cands) {
@@ -1043,7 +1093,7 @@ void autotune_levels(femh_handle* H, bool mg) {
     }
     L.variant = best_var;
     build_stencil_units(H, L, best);
-    H->tune_cache[key] = best * 4 + best_var;
+    H->tune_cache[key] = best * 16 + best_var;
   }
 }
 

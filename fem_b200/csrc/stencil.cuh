@@ -1261,6 +1261,7 @@ constexpr int kBulkSlots = 4;
 template <int NT, int OUT, int NZ>
 __global__ void __launch_bounds__(NT, 1)
 stencil2b_kernel(StencilArgs<float, float, float, float> a) {
+  static_assert(NZ > 0 && NZ % 4 == 0, "staged rows need a compile-time z extent, multiple of 4");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const StencilUnit un = a.units[blockIdx.x];
   const int rhs = blockIdx.y;
@@ -1280,10 +1281,11 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
   auto wrapy = [&](int j) { j %= ny; return j < 0 ? j + ny : j; };
   const int n1 = wrapy(un.j0 + 2 * t), n2 = wrapy(un.j0 + 2 * t + 1);
 
-  // stage layout (floats): U[3][NRU][nz], KC[NRK][nz], B[3][rows][nz], ID[rows][nz]
-  const int NRU = rows + 3, NRK = rows + 2;
-  const int oK = 3 * NRU * nz, oB = oK + NRK * nz, oI = oB + 3 * rows * nz;
-  const int SS = (oI + rows * nz + 3) & ~3;   // floats per stage, 16-byte multiple
+  // stage layout (floats), sized for the largest tile so that every offset is
+  // a compile-time constant: U[3][NRU][nz], KC[NRK][nz], B[3][RB][nz], ID[RB][nz]
+  constexpr int TRc = NT / NZ, RB = 2 * TRc - 1, NRU = RB + 3, NRK = RB + 2;
+  constexpr int oK = 3 * NRU * NZ, oB = oK + NRK * NZ, oI = oB + 3 * RB * NZ;
+  constexpr int SS = (oI + RB * NZ + 3) & ~3;   // floats per stage, 16-byte multiple
   const int PS = TR * 3 * nz;
   float* stg = reinterpret_cast<float*>(smem_raw);
   f2* QAB = reinterpret_cast<f2*>(stg + kBulkSlots * SS);   // [2][TR][3][nz]
@@ -1322,14 +1324,16 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
         done += n;
       }
     };
-    for (int c = 0; c < 3; ++c) seg(a.u + ((long long)rhs * 3 + c) * st + cd.off, 1, un.j0 - 1, NRU, c * NRU * nz);
-    seg(a.kc + cd.off, 0, un.j0 - 1, NRK, oK);
+    for (int c = 0; c < 3; ++c) seg(a.u + ((long long)rhs * 3 + c) * st + cd.off, 1, un.j0 - 1, rows + 3, c * NRU * nz);
+    seg(a.kc + cd.off, 0, un.j0 - 1, rows + 2, oK);
     if (OUT >= OUT_JACOBI) {
       for (int c = 0; c < 3; ++c)
-        seg(a.b + ((long long)rhs * 3 + c) * st + cd.off, -1, un.j0, rows, oB + c * rows * nz);
+        seg(a.b + ((long long)rhs * 3 + c) * st + cd.off, -1, un.j0, rows, oB + c * RB * nz);
       if (OUT != OUT_RESID) seg(a.invd + cd.off, -1, un.j0, rows, oI);
     }
   }
+  // plane of this lane's next copy (stage 0 is plane i0-2+lag), advanced per issue
+  int pl_next = ((un.i0 - 2 + plane_lag) % nx + nx) % nx;
   // stage g (= step g-1) is node plane i0-2+g of u, voxel plane i0-2+g of kc
   // and node plane i0-3+g of b / invd; lag = plane offset relative to i0-2+g.
   int issued = 0;   // stages issued so far (warp 0)
@@ -1342,12 +1346,10 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
       mbar_expect_tx(bar, tx_total);
     }
     __syncwarp();
-    if (bytes > 0) {
-      int pl = (un.i0 - 2 + g + plane_lag) % nx;
-      if (pl < 0) pl += nx;
-      bulk_g2s(smem_addr(stg + slot * SS + dst_off), src_base + 4LL * ((long long)pl * plane + src_off),
+    if (bytes > 0)
+      bulk_g2s(smem_addr(stg + slot * SS + dst_off), src_base + 4LL * ((long long)pl_next * plane + src_off),
                (unsigned)bytes, bar);
-    }
+    if (++pl_next == nx) pl_next = 0;
   };
   const int G = un.len + 3;   // stages 0 .. len+2 (step -1 .. len+1)
   if (tid == 0) {
@@ -1419,7 +1421,7 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const f2 bv = make_float2(own1 ? Bs[c * rows * nz + r1] : 0.f, own2 ? Bs[c * rows * nz + r2] : 0.f);
+        const f2 bv = make_float2(own1 ? Bs[c * RB * NZ + r1] : 0.f, own2 ? Bs[c * RB * NZ + r2] : 0.f);
         const f2 d = p_sub(bv, y[c]);
         if (OUT == OUT_RESID) {
           if (own1) ob[c * st + c1] = pin1 ? 0.f : d.x;
@@ -1449,6 +1451,8 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
       for (int q = 0; q < 4; ++q) car[c][q] = p_bc(0.f);
     }
   }
+  const int cellsz = nx * plane;
+  int pe_next = ((un.i0 - 1 + nx) % nx) * plane;   // voxel plane ie of step 0, advanced per step
   for (int s = 0; s <= un.len + 1; ++s) {
     const int g = s + 1;
     wait_stage(g);
@@ -1456,7 +1460,9 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
     if (abort_flag) break;
     if (tid < 32 && g + kBulkSlots - 1 < G) issue(g + kBulkSlots - 1);   // the slot of stage g-1
     const float* S = stg + (g % kBulkSlots) * SS;
-    const int pe = ((un.i0 - 1 + s + nx) % nx) * plane;   // voxel plane ie
+    const int pe = pe_next;   // voxel plane ie
+    pe_next += plane;
+    if (pe_next >= cellsz) pe_next -= cellsz;
     if (s >= 2 && live) gather((s - 1) & 1, S);
     if (s > un.len || !live) continue;
     f2 w[3][8];
@@ -1545,10 +1551,263 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
   }
 }
 
+// Scalar 2x2 Hadamard transform of a node patch and its inverse (same stage
+// order and signs as had4_fwd / had4_inv).
+template <typename T>
+__device__ __forceinline__ void had4s_fwd(T (&v)[4]) {
+  const T a0 = v[1] + v[0], a1 = v[1] - v[0], a2 = v[3] + v[2], a3 = v[3] - v[2];
+  v[0] = a2 + a0; v[2] = a2 - a0; v[1] = a3 + a1; v[3] = a3 - a1;
+}
+template <typename T>
+__device__ __forceinline__ void had4s_inv(T (&v)[4]) {
+  const T a0 = v[0] - v[2], a2 = v[0] + v[2], a1 = v[1] - v[3], a3 = v[1] + v[3];
+  v[0] = a0 - a1; v[1] = a0 + a1; v[2] = a2 - a3; v[3] = a2 + a3;
+}
+
+// FP64 operator, one voxel row per thread, inputs staged by bulk copies.
+// Schedule and staging of stencil2b_kernel (stage g = step g-1; u of node
+// plane ie+1, kc of voxel plane ie, b / invd of node plane ie-1), the
+// carried lower plane transformed in y and z and the upper-plane
+// contributions half transformed (as in stencilp_kernel), arithmetic in FP64.
+// Thread (r, z) streams voxel (i, j0-1+r, z); row 0 is the y halo.  Stage
+// layout: U[3][R+1][nz] (TIn), KC[R][nz], B[3][R-1][nz] (double), ID[R-1][nz]
+// (float); Q[2][R][3 corners][3][nz] doubles.
+template <int NT, int OUT, int NZ, typename TIn>
+__global__ void __launch_bounds__(NT, 1)
+stencil1b_kernel(StencilArgs<TIn, double, double, double> a) {
+  static_assert(NZ > 0 && NZ % 4 == 0, "staged rows need a compile-time z extent, multiple of 4");
+  constexpr int R = NT / NZ, NRU = R + 1, NRK = R, RB = R - 1;
+  constexpr int bU = 0, bK = bU + 3 * NRU * NZ * (int)sizeof(TIn), bB = bK + NRK * NZ * 8,
+                bI = bB + 3 * RB * NZ * 8;
+  constexpr int SSB = (bI + RB * NZ * 4 + 15) & ~15;   // bytes per stage
+  constexpr int QS = R * 9 * NZ;                       // doubles per Q buffer
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const StencilUnit un = a.units[blockIdx.x];
+  const int rhs = blockIdx.y;
+  const CellDesc cd = a.cells[un.cell];
+  if (a.stt && !a.stt[cd.id * kNumRhs + rhs].active) return;
+  const int nx = cd.nx, ny = cd.ny;
+  constexpr int nz = NZ;
+  const int tid = threadIdx.x;
+  const int r = tid / nz, z = tid - r * nz;
+  const int rows = un.rows;
+  const bool live = r <= rows;
+  const bool owner = live && r >= 1;
+  const int zp = (z + 1 == nz) ? 0 : z + 1;
+  const int zm = (z == 0) ? nz - 1 : z - 1;
+  auto wrapy = [&](int j) { j %= ny; return j < 0 ? j + ny : j; };
+  const int jr = wrapy(un.j0 - 1 + r);
+
+  unsigned char* stg = smem_raw;
+  double* Q = reinterpret_cast<double*>(stg + kBulkSlots * SSB);   // [2][R][3][3][nz]
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(Q + 2 * QS);
+  double* red = reinterpret_cast<double*>(bars + kBulkSlots);
+  __shared__ int abort_flag;
+  const int qrow = r * 9 * nz, qup = (r > 0 ? r - 1 : 0) * 9 * nz;
+
+  const long long st = a.ntot;
+  const int plane = ny * nz;
+  const int col = jr * nz + z;
+  double* obase = a.out + (long long)rhs * 3 * st + cd.off;
+
+  const char* src_base = nullptr;
+  int plane_lag = 0, src_off = 0, dst_off = 0, bytes = 0, esz = 0;
+  unsigned tx_total = 0;
+  if (tid < 32) {
+    int idx = 0;
+    auto seg = [&](const void* base, int es, int lag, int row0, int nrows, int dst) {
+      int done = 0;
+      while (done < nrows) {
+        const int r0 = wrapy(row0 + done);
+        const int n = min(nrows - done, ny - r0);
+        if (idx == tid) {
+          src_base = reinterpret_cast<const char*>(base);
+          esz = es;
+          plane_lag = lag;
+          src_off = r0 * nz;
+          dst_off = dst + done * nz * es;
+          bytes = n * nz * es;
+        }
+        tx_total += (unsigned)(n * nz * es);
+        ++idx;
+        done += n;
+      }
+    };
+    for (int c = 0; c < 3; ++c)
+      seg(a.u + ((long long)rhs * 3 + c) * st + cd.off, (int)sizeof(TIn), 1, un.j0 - 1, rows + 2,
+          bU + c * NRU * nz * (int)sizeof(TIn));
+    seg(a.kc + cd.off, 8, 0, un.j0 - 1, rows + 1, bK);
+    if (OUT >= OUT_JACOBI) {
+      for (int c = 0; c < 3; ++c) seg(a.b + ((long long)rhs * 3 + c) * st + cd.off, 8, -1, un.j0, rows, bB + c * RB * nz * 8);
+      if (OUT != OUT_RESID) seg(a.invd + cd.off, 4, -1, un.j0, rows, bI);
+    }
+  }
+  int pl_next = ((un.i0 - 2 + plane_lag) % nx + nx) % nx;
+  int issued = 0;
+  auto issue = [&](int g) {
+    issued = g + 1;
+    const int slot = g % kBulkSlots;
+    const unsigned bar = smem_addr(bars + slot);
+    if (tid == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(bar, tx_total);
+    }
+    __syncwarp();
+    if (bytes > 0)
+      bulk_g2s(smem_addr(stg + slot * SSB + dst_off), src_base + (long long)esz * ((long long)pl_next * plane + src_off),
+               (unsigned)bytes, bar);
+    if (++pl_next == nx) pl_next = 0;
+  };
+  const int G = un.len + 3;
+  if (tid == 0) {
+    for (int k = 0; k < kBulkSlots; ++k) mbar_init(smem_addr(bars + k), 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid < 32)
+    for (int g = 0; g < kBulkSlots && g < G; ++g) issue(g);
+  int waited = 0;
+  auto wait_stage = [&](int g) {
+    if (!mbar_wait(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1))) {
+      if (a.err) atomicExch(a.err, 1);
+      abort_flag = 1;
+    }
+    waited = g + 1;
+  };
+
+  double prv[3][4], car[3][4];
+  double own[3] = {0, 0, 0}, unode[3] = {0, 0, 0}, rawn[3] = {0, 0, 0};
+  int pg = 0;
+  double acc = 0.0;
+  auto patch = [&](const unsigned char* S, double (&h)[3][4], double (&mine)[3]) {
+    const TIn* U = reinterpret_cast<const TIn*>(S + bU);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const TIn* Uc = U + c * NRU * nz + r * nz;
+      mine[c] = (double)Uc[z];
+      h[c][0] = mine[c];
+      h[c][1] = (double)Uc[zp];
+      h[c][2] = (double)Uc[nz + z];
+      h[c][3] = (double)Uc[nz + zp];
+      had4s_fwd(h[c]);
+    }
+  };
+  auto gather = [&](int buf, const unsigned char* S) {
+    const double* Qg = Q + buf * QS;
+    double* ob = obase + pg + col;
+    const int rb = (r - 1) * nz + z;   // owned row in the b / invd arrays
+    const bool pin = (pg + col == 0);
+    double idv = 0.0;
+    if (OUT == OUT_JACOBI || OUT == OUT_JACOBI_DOT) idv = (double)reinterpret_cast<const float*>(S + bI)[rb];
+    const double* Bs = reinterpret_cast<const double*>(S + bB);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double y = own[c] + Qg[qrow + (0 * 3 + c) * nz + zm] + Qg[qup + (1 * 3 + c) * nz + z] +
+                       Qg[qup + (2 * 3 + c) * nz + zm];
+      if (OUT == OUT_APPLY || OUT == OUT_APPLY_DOT) {
+        ob[c * st] = y;
+        if (OUT == OUT_APPLY_DOT) acc += unode[c] * y;
+      } else {
+        const double bv = Bs[c * RB * nz + rb];
+        if (OUT == OUT_RESID) {
+          ob[c * st] = pin ? 0.0 : bv - y;
+        } else {
+          const double xv = unode[c] + a.omega * idv * (bv - y);
+          ob[c * st] = xv;
+          if (OUT == OUT_JACOBI_DOT) acc += xv * bv;
+        }
+      }
+    }
+  };
+
+  wait_stage(0);
+  if (live) {
+    double mine[3];
+    patch(stg, prv, mine);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      rawn[c] = mine[c];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) car[c][q] = 0.0;
+    }
+  }
+  const int cellsz = nx * plane;
+  int pe_next = ((un.i0 - 1 + nx) % nx) * plane;
+  for (int s = 0; s <= un.len + 1; ++s) {
+    const int g = s + 1;
+    wait_stage(g);
+    __syncthreads();
+    if (abort_flag) break;
+    if (tid < 32 && g + kBulkSlots - 1 < G) issue(g + kBulkSlots - 1);
+    const unsigned char* S = stg + (g % kBulkSlots) * SSB;
+    const int pe = pe_next;
+    pe_next += plane;
+    if (pe_next >= cellsz) pe_next -= cellsz;
+    if (s >= 2 && owner) gather((s - 1) & 1, S);
+    if (s > un.len || !live) continue;
+    double w[3][8];
+    double cur0[3];
+    {
+      double cur[3][4];
+      patch(S, cur, cur0);
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          w[c][q] = cur[c][q] + prv[c][q];
+          w[c][4 + q] = cur[c][q] - prv[c][q];
+          prv[c][q] = cur[c][q];
+        }
+    }
+    had_block(w, a.k, reinterpret_cast<const double*>(S + bK)[r * nz + z]);
+    double* Qb = Q + (s & 1) * QS;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double tot[4];
+      tot[0] = car[c][0] - w[c][4];
+      car[c][0] = w[c][4];
+#pragma unroll
+      for (int q = 1; q < 4; ++q) {
+        tot[q] = (w[c][q] - w[c][4 + q]) + car[c][q];
+        car[c][q] = w[c][q] + w[c][4 + q];
+      }
+      had4s_inv(tot);
+      own[c] = tot[0];
+      unode[c] = rawn[c];
+      rawn[c] = cur0[c];
+      if (s > 0) {
+        Qb[qrow + (0 * 3 + c) * nz + z] = tot[1];   // node (jr, z+1)
+        Qb[qrow + (1 * 3 + c) * nz + z] = tot[2];   // node (jr+1, z)
+        Qb[qrow + (2 * 3 + c) * nz + z] = tot[3];   // node (jr+1, z+1)
+      }
+    }
+    pg = pe;
+  }
+  if (tid == 0) {
+    for (int g = waited; g < issued; ++g)
+      if (!mbar_wait(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1))) break;
+  }
+  if (OUT == OUT_APPLY_DOT || OUT == OUT_JACOBI_DOT) {
+    double v[1] = {acc};
+    block_reduce<1>(v, red);
+    if (tid == 0) a.partials[(long long)un.slot * kNumRhs + rhs] = v[0];
+  }
+}
+
+// Shared memory bytes of one stencil1b_kernel CTA.
+inline size_t stencil1b_smem_bytes(int NT, int nz, int in_size) {
+  const int R = NT / nz;
+  const size_t stage = ((size_t)3 * (R + 1) * nz * in_size + (size_t)R * nz * 8 + (size_t)3 * (R - 1) * nz * 8 +
+                        (size_t)(R - 1) * nz * 4 + 15) & ~(size_t)15;
+  return kBulkSlots * stage + sizeof(double) * 2 * (size_t)R * 9 * nz + sizeof(unsigned long long) * kBulkSlots +
+         64 * sizeof(double);
+}
+
 // Shared memory bytes of one stencil2b_kernel CTA (tiles of up to 2*TR-1 rows).
 inline size_t stencil2b_smem_bytes(int NT, int nz) {
   const int TR = NT / nz, rows = 2 * TR - 1;
-  const size_t SS = ((size_t)(3 * (rows + 3) + (rows + 2) + 4 * rows) * nz + 3) & ~(size_t)3;
+  const size_t SS = ((size_t)(3 * (rows + 3) + (rows + 2) + 4 * rows) * nz + 3) & ~(size_t)3;   // as in the kernel
   return sizeof(float) * kBulkSlots * SS + sizeof(f2) * 4 * (size_t)TR * 3 * nz +
          sizeof(unsigned long long) * kBulkSlots + 64 * sizeof(double);
 }

@@ -82,7 +82,11 @@ typedef struct {
   int stencil_variant;    /* 0: chosen by the autotuner; else forced: 1 one voxel row per
                              thread, 2 two rows per thread, 3 two load cases per thread in
                              packed FP32x2 lanes, 4 two rows per thread in packed FP32x2
-                             lanes (3 and 4: FP32 operators; FP64 ones use 1 and 2) */
+                             lanes, 5 as 4 with the inputs staged in shared memory by bulk
+                             copies (3-5: FP32 operators; FP64 ones use 1 or 2), 6 one row
+                             per thread in FP64 with staged inputs (FP64 operators; FP32
+                             ones use 1).  5 and 6 need a z extent in {16,24,32,48,64,128
+                             (,256 for 6)}; elsewhere 4 and 1 run instead */
 } femh_config;
 
 typedef struct {

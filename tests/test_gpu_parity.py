@@ -61,6 +61,33 @@ def test_fp32_stencil_variants_match_oracle(femh, oracle, rng, shape, variant):
     assert _rel(y, yo) < TOL_APPLY32
 
 
+@pytest.mark.parametrize("shape", [(8, 16, 128), (6, 20, 64), (4, 32, 32), (5, 11, 128)])
+def test_fp64_staged_apply_matches_oracle(femh, oracle, rng, shape):
+    """The FP64 kernel with bulk-copy staged inputs (forced; these shapes meet
+    its row condition) against the oracle operator at the FP64 bar."""
+    rho = rng.random(shape)
+    u = rng.standard_normal((6,) + shape + (3,))
+    e = femh.Engine(solver=femh.JACOBI_PCG, stencil_variant=6, autotune=0)
+    y = e.apply_operator(rho, u)
+    mat = oracle.material()
+    yo = oracle.apply(shape, oracle.k0(1.0, 0.3, 1.0 / shape[0]), oracle.coef(mat, rho), u)
+    assert _rel(y, yo) < TOL_APPLY
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed_pc"])
+def test_staged_kernels_C_matches_oracle(femh, oracle, precision):
+    """C^H with the staged kernels forced (FP64 operator: variant 6; the FP32
+    multigrid levels fall back where a level does not qualify)."""
+    from fem_b200 import fields
+    rho = fields.smooth_cell(64, sigma=3.0, seed=12)[:16, :24, :].copy()
+    Co, *_ = oracle.homogenize(rho)
+    prec = femh.FP64 if precision == "fp64" else femh.MIXED_PC
+    e = femh.Engine(precision=prec, stencil_variant=6)
+    C, info = e.homogenize(rho)
+    assert info["status"] == 0 and max(info["rel_residual"]) < 1e-10
+    assert _rel(C, Co) < (TOL_FP64 if precision == "fp64" else TOL_MIXED)
+
+
 @pytest.mark.parametrize("bf16", [0, 1])
 @pytest.mark.parametrize("shape", [(16, 16, 16), (16, 8, 24)])
 def test_mixed_pc_C_matches_oracle(femh, oracle, shape, bf16):
