@@ -1171,6 +1171,14 @@ bool fuse_rz(const femh_handle* H) {
 // must already hold the first damped-Jacobi sweep omega*invd*r0 (written by
 // the CG update kernel).  Buffer roles are fixed by the sweep counts, so the
 // launch sequence is identical every iteration (graph capture).
+// Profile name of a per-level kernel ("<base>_L<level>"), interned in the
+// handle's statistics map so that the pointer stays valid.
+const char* level_name(femh_handle* H, const char* base, int level) {
+  if (!H->prof) return base;
+  const std::string k = std::string(base) + "_L" + std::to_string(level);
+  return H->kstats.emplace(k, femh_handle::KStat{}).first->first.c_str();
+}
+
 template <typename TM, typename TMC, typename TB>
 void vcycle_level_down(femh_handle* H, int l, const TB* b, TM* cur, TM* oth, TM* sol) {
   const femh_config& c = H->cfg;
@@ -1187,7 +1195,7 @@ void vcycle_level_down(femh_handle* H, int l, const TB* b, TM* cur, TM* oth, TM*
   }
   if (L.smooth.su.empty()) return;
   if (l > 0) {
-    Prof prof_(H, "k_jacobi0", 0.0);
+    Prof prof_(H, level_name(H, "k_jacobi0", l), 18.0 * (sizeof(TB) + sizeof(TM)) * L.nodes_smooth);
     k_jacobi0<TB, TM><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, L.smooth.d_nu, b, cur, (TM*)nullptr, L.invd, om, stt,
                                                           L.ntot);
     LAUNCH_CHECK(H);
@@ -1198,7 +1206,7 @@ void vcycle_level_down(femh_handle* H, int l, const TB* b, TM* cur, TM* oth, TM*
   }
   stencil<TM, OUT_RESID>(H, L, true, (const TM*)cur, oth, b, (const TMC*)L.kc, nullptr, stt, om);
   Level& C = H->levels[l + 1];
-  Prof prof_(H, "k_restrict", 0.0);
+  Prof prof_(H, level_name(H, "k_restrict", l), 18.0 * sizeof(TM) * (L.nodes_smooth + C.ntot));
   k_restrict<TM, TM><<<NODE_GRID(C.all), 256, 0, s>>>(L.d_cells, C.d_cells, C.all.d_nu, oth, (TM*)C.bv, stt,
                                                       L.ntot, C.ntot);
   LAUNCH_CHECK(H);
@@ -1213,7 +1221,7 @@ void vcycle_level_up(femh_handle* H, int l, const TB* b, TM* x, TM* t, const TM*
   if (L.smooth.su.empty()) return;
   Level& C = H->levels[l + 1];
   {
-    Prof prof_(H, "k_prolong_add", 0.0);
+    Prof prof_(H, level_name(H, "k_prolong_add", l), 18.0 * sizeof(TM) * (2.0 * L.nodes_smooth + C.ntot));
     k_prolong_add<TM, TM><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, C.d_cells, L.smooth.d_nu, x, coarse_sol,
                                                               stt, L.ntot, C.ntot);
     LAUNCH_CHECK(H);
@@ -1293,7 +1301,9 @@ void pcg_iteration(femh_handle* H, const typename PR::K* kcg) {
     LAUNCH_CHECK(H);
   }
   {
-    Prof prof_(H, "k_cg_update", 0.0);
+    Prof prof_(H, "k_cg_update",
+               (18.0 * (5 * sizeof(TV) + sizeof(TP) + (gmg ? sizeof(TM) : 0) + (rm ? sizeof(TM) : 0)) + 4.0) *
+                   (double)L0.ntot);
     k_cg_update<TV, TP, TV, TM><<<NODE_GRID(L0.all), 256, 0, s>>>(
         L0.d_cells, L0.all.d_nu, x, r, p, q, L0.invd, gmg ? (TM*)L0.xa : (TM*)nullptr, rm, c.omega, stt,
         H->d_part_n, L0.ntot);
@@ -1318,7 +1328,7 @@ void pcg_iteration(femh_handle* H, const typename PR::K* kcg) {
     LAUNCH_CHECK(H);
   }
   {
-    Prof prof_(H, "k_cg_dir", 0.0);
+    Prof prof_(H, "k_cg_dir", 18.0 * (sizeof(TM) + 2 * sizeof(TP)) * (double)L0.ntot);
     k_cg_dir<TP, TM, TV><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, p, (const TM*)z,
                                                            (const TV*)r, L0.invd, stt, L0.ntot);
     LAUNCH_CHECK(H);
