@@ -299,6 +299,7 @@ struct femh_handle {
   double* d_out = nullptr;      // gradient / dCdrho output [21][nvox]
   double* d_nrm = nullptr;      // [ncells][6]
   bool solved = false;
+  bool have_x = false;   // x64 holds the last solution of these cells (warm starts)
   std::vector<double> C_last;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -694,6 +695,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   H->setup.release();
   H->levels.clear();
   H->solved = false;
+  H->have_x = false;
   Arena& ar = H->setup;
   cudaStream_t s = H->stream;
   const int nc = (int)shapes.size() / 3;
@@ -1336,8 +1338,11 @@ void pcg_iteration(femh_handle* H, const typename PR::K* kcg) {
 }
 
 // PCG on K x = scale*b for every (cell, rhs) whose state is active.
+// warm: x already holds the starting iterate and b is its residual; the
+// relative residual is measured against ||b_orig||^2 in H->d_nrm.
 template <class PR, typename TB>
-void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, double tol, int iters_out[]) {
+void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, double tol, int iters_out[],
+         bool warm = false) {
   using TV = typename PR::V;
   using TP = typename PR::P;
   using TM = typename PR::M;
@@ -1361,12 +1366,13 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
   {
     Prof prof_(H, "k_cg_init", 0.0);
     k_cg_init<TB, TV, TP><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, b, x, r, p, L0.invd, stt,
-                                                            H->d_part_n, L0.ntot, gmg ? 0 : 1);
+                                                            H->d_part_n, L0.ntot, gmg ? 0 : 1, warm ? 1 : 0);
     LAUNCH_CHECK(H);
   }
   {
     Prof prof_(H, "k_fin_init", 0.0);
-    k_fin_init<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_n, nc, gmg ? 0 : 1);
+    k_fin_init<<<fin_blocks(nc), 128, 0, s>>>(stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_n, nc, gmg ? 0 : 1,
+                                              warm ? H->d_nrm : nullptr);
     LAUNCH_CHECK(H);
   }
   if (gmg) {
@@ -1532,28 +1538,42 @@ void solve_all(femh_handle* H, std::vector<femh_solve_info>& infos) {
   std::vector<double> rn2;
   int outer_done = 0;
   std::vector<int> final_status(nc * kNumRhs, CG_CONVERGED);
+  // warm start: the previous solution of this handle (same cells) is the
+  // starting iterate; its residual b - K x0 replaces b (d_nrm keeps ||b||^2)
+  const bool warm = c.warm_start && H->have_x;
   if (c.precision == FEMH_FP64 || c.precision == FEMH_MIXED_PC) {
     for (auto& S : H->state) {
       S = CGState{};
       S.active = 1;
       S.scale = 1.0;
     }
+    const double* b0 = H->b64;
+    if (warm) {
+      double* r0 = (double*)H->cg_q;   // free until the first CG apply
+      stencil<double, OUT_RESID>(H, L0, false, (const double*)H->x64, r0, (const double*)H->b64,
+                                 (const double*)H->kc64, nullptr, nullptr, 0.0);
+      b0 = r0;
+    }
     if (c.precision == FEMH_FP64)
-      pcg<Prec<double, double, double, double, double>>(H, H->b64, H->kc64, c.max_iter, c.tol, iters.data());
+      pcg<Prec<double, double, double, double, double>>(H, b0, H->kc64, c.max_iter, c.tol, iters.data(), warm);
     else if (c.store_bf16)   // FP64 CG and operator, FP32 multigrid, bf16 search directions
-      pcg<Prec<double, __nv_bfloat16, double, float, float>>(H, H->b64, H->kc64, c.max_iter, c.tol, iters.data());
+      pcg<Prec<double, __nv_bfloat16, double, float, float>>(H, b0, H->kc64, c.max_iter, c.tol, iters.data(), warm);
     else   // FP64 CG and operator, FP32 multigrid preconditioner and search directions
-      pcg<Prec<double, float, double, float, float>>(H, H->b64, H->kc64, c.max_iter, c.tol, iters.data());
+      pcg<Prec<double, float, double, float, float>>(H, b0, H->kc64, c.max_iter, c.tol, iters.data(), warm);
     for (int t = 0; t < nc * kNumRhs; ++t) final_status[t] = H->state[t].status;
     outer_done = 1;
     true_residual(H, rn2);
   } else {
-    CK(cudaMemsetAsync(H->x64, 0, sizeof(double) * 18 * H->nvox, s));
-    CK(cudaMemcpyAsync(H->r64, H->b64, sizeof(double) * 18 * H->nvox, cudaMemcpyDeviceToDevice, s));
-    rn2 = bn2;
+    if (warm) {   // defect correction continues from the previous solution
+      true_residual(H, rn2);
+    } else {
+      CK(cudaMemsetAsync(H->x64, 0, sizeof(double) * 18 * H->nvox, s));
+      CK(cudaMemcpyAsync(H->r64, H->b64, sizeof(double) * 18 * H->nvox, cudaMemcpyDeviceToDevice, s));
+      rn2 = bn2;
+    }
     std::vector<int> outer_on(nc * kNumRhs, 1);
     for (int t = 0; t < nc * kNumRhs; ++t)
-      if (!(bn2[t] > 0.0)) outer_on[t] = 0;
+      if (!(bn2[t] > 0.0) || (warm && std::sqrt(rn2[t] / bn2[t]) < c.tol)) outer_on[t] = 0;
     for (int o = 0; o < c.max_outer; ++o) {
       bool any = false;
       for (int t = 0; t < nc * kNumRhs; ++t) {
@@ -1673,6 +1693,7 @@ void run_cells(femh_handle* H, const std::vector<int>& shapes, const std::vector
   }
   solve_all(H, infos);
   check_kernel_error(H);
+  H->have_x = true;
   std::vector<double> dens;
   energy_C(H, C, dens);
   for (int i = 0; i < H->ncells; ++i) infos[i].density = dens[i];
@@ -1755,6 +1776,7 @@ femh_status femh_config_default(femh_config* c) {
   c->coarse_avg = 0;
   c->autotune = 1;
   c->stencil_variant = 0;
+  c->warm_start = 0;
   return FEMH_OK;
 }
 
@@ -2001,6 +2023,7 @@ femh_status femh_apply_operator(femh_handle* H, int nx, int ny, int nz, double h
       LAUNCH_CHECK(H);
     }
     double* tmp = H->d_out;
+    H->have_x = false;   // x64 serves as the input buffer below
     CK(cudaMemcpyAsync(tmp, u, sizeof(double) * 18 * nn, k_in, s));
     {
       Prof prof_(H, "k_layout", 0.0);

@@ -148,13 +148,14 @@ __global__ void k_rhs(const CellDesc* cells, const NodeUnit* units, const double
 }
 
 // ------------------------------------------------------------- CG pieces ---
-// Start of PCG: x = 0, r = s*b (s = per (cell,rhs) scale), partial ||r||^2.
+// Start of PCG: x = 0 (kept as it is when keep_x: a warm start, with b the
+// residual of that x), r = s*b (s = per (cell,rhs) scale), partial ||r||^2.
 // With jacobi != 0 also partial r.(invd r) for the Jacobi-preconditioned rz and
 // p = invd r.  Partials: [slot][6][2].
 template <typename TB, typename TV, typename TP>
 __global__ void k_cg_init(const CellDesc* cells, const NodeUnit* units, const TB* __restrict__ b, TV* __restrict__ x, TV* __restrict__ r,
                           TP* __restrict__ p, const float* __restrict__ invd, const CGState* stt, double* __restrict__ part, long long ntot,
-                          int jacobi) {
+                          int jacobi, int keep_x) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cd = cells[u.cell];
@@ -169,7 +170,7 @@ __global__ void k_cg_init(const CellDesc* cells, const NodeUnit* units, const TB
       for (int c = 0; c < 3; ++c) {
         const long long o = ((long long)rhs * 3 + c) * ntot + g;
         const double rv = (n == 0) ? 0.0 : S.scale * (double)ld_val(b + o);
-        st_val(x + o, 0.0);
+        if (!keep_x) st_val(x + o, 0.0);
         st_val(r + o, rv);
         v[0] += rv * rv;
         const double z = (double)id * rv;
@@ -275,18 +276,20 @@ __device__ __forceinline__ double sum_slots(const double* part, int b, int e, in
 
 // After k_cg_init: bnorm2, rz (Jacobi) / rr; decide which (cell, rhs) run.
 // One thread per (cell, rhs).
+// bn2 != nullptr (warm start): ||b||^2 per (cell, rhs), against which the
+// residual of the starting x is measured; else the start is x = 0 and r = b.
 __global__ void k_fin_init(CGState* stt, const int* slot_begin, const int* slot_end,
-                           const double* part, int ncells, int jacobi) {
+                           const double* part, int ncells, int jacobi, const double* bn2) {
   FIN_PROLOGUE
   CGState S = stt[t];
   if (!S.active) return;
   const double rr = sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 2, 0);
-  S.bnorm2 = rr;
+  S.bnorm2 = bn2 ? bn2[t] : rr;
   S.rr = rr;
   S.rz = jacobi ? sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 2, 1) : 0.0;
   S.iters = 0;
-  S.rel = (rr > 0.0) ? 1.0 : 0.0;
-  if (!(rr > 0.0)) { S.active = 0; S.status = CG_CONVERGED; }
+  S.rel = (S.bnorm2 > 0.0) ? sqrt(rr / S.bnorm2) : 0.0;
+  if (!(S.bnorm2 > 0.0) || !(rr > 0.0) || S.rel < S.tol) { S.active = 0; S.status = CG_CONVERGED; }
   if (lead) stt[t] = S;
 }
 

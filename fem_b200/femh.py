@@ -54,7 +54,7 @@ class _Config(ctypes.Structure):
         ("tol", ctypes.c_double), ("max_iter", ctypes.c_int),
         ("inner_tol", ctypes.c_double), ("max_outer", ctypes.c_int),
         ("store_bf16", ctypes.c_int), ("graph_chunk", ctypes.c_int), ("coarse_avg", ctypes.c_int),
-        ("autotune", ctypes.c_int), ("stencil_variant", ctypes.c_int),
+        ("autotune", ctypes.c_int), ("stencil_variant", ctypes.c_int), ("warm_start", ctypes.c_int),
     ]
 
 
@@ -136,6 +136,7 @@ class Config:
     coarse_avg: int = 0
     autotune: int = 1
     stencil_variant: int = 0
+    warm_start: int = 0
 
     def to_c(self) -> _Config:
         c = _Config()

@@ -56,6 +56,7 @@ void FEM3DFun::ensure_handle() {
   c.rho_max = 1.0;
   c.precision = precision;
   c.solver = solver;
+  c.warm_start = warmStart ? 1 : 0;
   check(nullptr, femh_create(&h_, &c));
 }
 

@@ -78,6 +78,9 @@ class FEM3DFun : public RealFun {
   // material of the solid (fast_fem: ElasticMaterial(E, nu)), precision/solver
   double E = 1.0, nu = 0.3;
   int precision = FEMH_FP64, solver = FEMH_GMG_PCG;
+  // start each solve from the previous one's fluctuation fields (consecutive
+  // setParam calls of a line search / descent differ little); off by default
+  bool warmStart = false;
 
   std::array<double, 36> G{}, G0{}, wG{};
   double density = 0, m0 = 0, mw = 0;

@@ -65,7 +65,7 @@ typedef struct {
   double E_s, E_min, penal, nu;
   double bin_hi, bin_lo;
   double rho_min, rho_max; /* clamp applied before the law (fast_fem clamps 1e-3..1) */
-  int precision;          /* FEMH_FP64 | FEMH_MIXED */
+  int precision;          /* FEMH_FP64 | FEMH_MIXED | FEMH_MIXED_PC */
   int solver;             /* FEMH_JACOBI_PCG | FEMH_GMG_PCG */
   int pre_smooth, post_smooth; /* damped-Jacobi sweeps per level (GMG) */
   double omega;           /* Jacobi damping */
@@ -87,6 +87,10 @@ typedef struct {
                              per thread in FP64 with staged inputs (FP64 operators; FP32
                              ones use 1).  5 and 6 need a z extent in {16,24,32,48,64,128
                              (,256 for 6)}; elsewhere 4 and 1 run instead */
+  int warm_start;         /* 1: a solve on the same cells as the handle's previous solve
+                             starts from that solution (chi) instead of zero -- the
+                             line-search / descent case of fast_fem/run3d.cpp:238-289;
+                             results agree with a cold start within the tolerance */
 } femh_config;
 
 typedef struct {
