@@ -206,6 +206,11 @@ struct UnitList {
   NodeUnit* d_nu = nullptr;
 };
 
+// Stencil units of one z extent: entries [b, e) of a unit list sorted by z extent.
+struct UnitGroups {
+  std::vector<int> nz, b, e;
+};
+
 struct Level {
   std::vector<CellDesc> cells;
   CellDesc* d_cells = nullptr;
@@ -217,6 +222,11 @@ struct Level {
   int variant = 2;   // stencil kernel (femh_config::stencil_variant numbering)
   bool bulk_ok = false;     // the bulk-copy staged FP32 kernel (variant 5) can run on this level
   bool bulk_ok64 = false;   // the bulk-copy staged FP64 kernel (variant 6) can run on this level
+  // cells of several z extents, each one with a compile-time kernel (a batch
+  // of uneven cells): the unit lists are sorted by z extent and each extent
+  // launches its own specialised kernel
+  bool grouped = false;
+  UnitGroups gall, gsmooth, g64;
   // level 0 of the mixed modes also runs FP64 operator applies (CG / true
   // residual): they get their own tuned layout (FP64 kernels spill in the
   // layout that suits FP32)
@@ -438,6 +448,38 @@ int variant_nt(int level_nt, int maxnz, int variant) {
   return level_nt;
 }
 
+// z extents with compile-time kernels, and their threads per CTA.
+bool spec_nz(int nz) { return nz == 16 || nz == 24 || nz == 32 || nz == 48 || nz == 64 || nz == 128 || nz == 256; }
+int spec_nt(int nz) { return (nz == 24 || nz == 48) ? 480 : 512; }
+
+// Threads per CTA that a cell's stencil units are cut for.
+int cell_nt(const Level& L, const CellDesc& cd, int variant) {
+  return L.grouped ? variant_nt(spec_nt(cd.nz), cd.nz, variant) : variant_nt(L.NT, L.maxnz, variant);
+}
+
+// On grouped levels: sort a unit list by z extent (stable, so each cell's
+// units stay in order; slots travel with their units) and record the groups.
+void group_units(const Level& L, std::vector<StencilUnit>& su, UnitGroups& g, bool sort) {
+  g.nz.clear();
+  g.b.clear();
+  g.e.clear();
+  if (!L.grouped) return;
+  if (sort)
+    std::stable_sort(su.begin(), su.end(), [&](const StencilUnit& x, const StencilUnit& y) {
+      return L.cells[x.cell].nz < L.cells[y.cell].nz;
+    });
+  for (int i = 0; i < (int)su.size(); ++i) {
+    const int nz = L.cells[su[i].cell].nz;
+    if (g.nz.empty() || g.nz.back() != nz) {
+      g.nz.push_back(nz);
+      g.b.push_back(i);
+      g.e.push_back(i + 1);
+    } else {
+      g.e.back() = i + 1;
+    }
+  }
+}
+
 }  // namespace
 
 // ======================================================== kernel launch ===
@@ -566,11 +608,6 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
     const double kv[8] = {k.A, k.Bd - k.Bo, k.Bo, k.D1 - k.O1, k.O1, k.D2 - k.O2, k.O2, k.G};
     for (int i = 0; i < 8; ++i) a.kp[i] = make_float2((float)kv[i], (float)kv[i]);
   }
-  const size_t smem =
-      variant == 3 ? sizeof(float4) * 12 * (size_t)L.NT + 2 * sizeof(float2) * (size_t)(12 * L.NT + 3 * L.maxnz) +
-                           64 * sizeof(double)
-      : variant == 2 ? sizeof(T) * (size_t)(2 * (6 * L.NT + 3 * L.maxnz) + 24 * L.NT) + 16 + 64 * sizeof(double)
-                     : 2 * sizeof(T) * (size_t)(15 * L.NT + 3 * L.maxnz) + 16 + 64 * sizeof(double);
   dim3 grid((unsigned)units.size(), kNumRhs);
   static const char* mode_names[] = {"apply", "apply_dot", "jacobi", "jacobi_dot", "resid"};
   char nm[64];
@@ -592,82 +629,102 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   if (OUT >= OUT_JACOBI) per += 18.0 * sizeof(TB) + (OUT == OUT_RESID ? 0.0 : 4.0);
   std::string key(nm);
   Prof prof_(H, H->prof ? H->kstats.emplace(key, femh_handle::KStat{}).first->first.c_str() : nm, nodes * per);
-  if constexpr (std::is_same<T, double>::value && std::is_same<TOut, double>::value &&
-                std::is_same<TB, double>::value && std::is_same<TC, double>::value &&
-                (std::is_same<TIn, double>::value || std::is_same<TIn, float>::value)) {
-    if (variant == 6) {
-      const size_t sm6 = stencil1b_smem_bytes(L.NT, L.nz_spec, (int)sizeof(TIn));
-      switch (L.nz_spec) {
-        case 16: stencil_go6<512, OUT, 16>(H, grid, sm6, a); return;
-        case 24: stencil_go6<480, OUT, 24>(H, grid, sm6, a); return;
-        case 32: stencil_go6<512, OUT, 32>(H, grid, sm6, a); return;
-        case 48: stencil_go6<480, OUT, 48>(H, grid, sm6, a); return;
-        case 64: stencil_go6<512, OUT, 64>(H, grid, sm6, a); return;
-        case 128: stencil_go6<512, OUT, 128>(H, grid, sm6, a); return;
-        case 256: stencil_go6<512, OUT, 256>(H, grid, sm6, a); return;
-        default: throw FemhError{FEMH_E_ARG, "staged FP64 stencil on an ineligible level"};
-      }
-    }
-  }
-  if constexpr (std::is_same<TIn, float>::value && std::is_same<TOut, float>::value &&
-                std::is_same<TB, float>::value && std::is_same<TC, float>::value) {
-    if (variant == 5) {   // eligible levels have a compile-time z extent and 384-thread tiles
-      const int nt = variant_nt(L.NT, L.maxnz, 5);
-      const size_t sm5 = stencil2b_smem_bytes(nt, L.nz_spec);
-      switch (L.nz_spec) {
-        case 16: stencil_go5<384, OUT, 16>(H, grid, sm5, a); return;
-        case 24: stencil_go5<384, OUT, 24>(H, grid, sm5, a); return;
-        case 32: stencil_go5<384, OUT, 32>(H, grid, sm5, a); return;
-        case 48: stencil_go5<384, OUT, 48>(H, grid, sm5, a); return;
-        case 64: stencil_go5<384, OUT, 64>(H, grid, sm5, a); return;
-        case 128: stencil_go5<384, OUT, 128>(H, grid, sm5, a); return;
-        default: throw FemhError{FEMH_E_ARG, "bulk-copy stencil on an ineligible level"};
-      }
-    }
-  }
-  if constexpr (std::is_same<T, float>::value) {
-    if (variant == 4) {
-      const int nt = variant_nt(L.NT, L.maxnz, 4);
-      const size_t sm4 =
-          sizeof(float2) * 18 * (size_t)nt + sizeof(float) * (6 * (size_t)L.maxnz + 2) + 64 * sizeof(double);
-      if (nt == 384) {
-        switch (L.nz_spec) {
-          case 16: stencil_go4<384, OUT, 16>(H, grid, sm4, a); return;
-          case 24: stencil_go4<384, OUT, 24>(H, grid, sm4, a); return;
-          case 32: stencil_go4<384, OUT, 32>(H, grid, sm4, a); return;
-          case 48: stencil_go4<384, OUT, 48>(H, grid, sm4, a); return;
-          case 64: stencil_go4<384, OUT, 64>(H, grid, sm4, a); return;
-          case 128: stencil_go4<384, OUT, 128>(H, grid, sm4, a); return;
-          default: stencil_go4<384, OUT, 0>(H, grid, sm4, a); return;
+  // launch on units of one z extent (nz_spec > 0: compile-time kernels) or on
+  // the level's runtime-z kernels (nz_spec = 0), lnt threads per CTA
+  auto launch = [&](int nz_spec, int lnt, int maxnz, dim3 grid, const StencilArgs<TIn, TOut, TB, TC>& a) {
+    const size_t smem =
+        variant == 3 ? sizeof(float4) * 12 * (size_t)lnt + 2 * sizeof(float2) * (size_t)(12 * lnt + 3 * maxnz) +
+                             64 * sizeof(double)
+        : variant == 2 ? sizeof(T) * (size_t)(2 * (6 * lnt + 3 * maxnz) + 24 * lnt) + 16 + 64 * sizeof(double)
+                       : 2 * sizeof(T) * (size_t)(15 * lnt + 3 * maxnz) + 16 + 64 * sizeof(double);
+    if constexpr (std::is_same<T, double>::value && std::is_same<TOut, double>::value &&
+                  std::is_same<TB, double>::value && std::is_same<TC, double>::value &&
+                  (std::is_same<TIn, double>::value || std::is_same<TIn, float>::value)) {
+      if (variant == 6) {
+        const size_t sm6 = stencil1b_smem_bytes(lnt, nz_spec, (int)sizeof(TIn));
+        switch (nz_spec) {
+          case 16: stencil_go6<512, OUT, 16>(H, grid, sm6, a); return;
+          case 24: stencil_go6<480, OUT, 24>(H, grid, sm6, a); return;
+          case 32: stencil_go6<512, OUT, 32>(H, grid, sm6, a); return;
+          case 48: stencil_go6<480, OUT, 48>(H, grid, sm6, a); return;
+          case 64: stencil_go6<512, OUT, 64>(H, grid, sm6, a); return;
+          case 128: stencil_go6<512, OUT, 128>(H, grid, sm6, a); return;
+          case 256: stencil_go6<512, OUT, 256>(H, grid, sm6, a); return;
+          default: throw FemhError{FEMH_E_ARG, "staged FP64 stencil on an ineligible level"};
         }
       }
-      if (L.nz_spec == 256) {
-        stencil_go4<512, OUT, 256>(H, grid, sm4, a);
-        return;
-      }
-      switch (nt) {
-        case 128: stencil_go4<128, OUT, 0>(H, grid, sm4, a); return;
-        case 256: stencil_go4<256, OUT, 0>(H, grid, sm4, a); return;
-        case 512: stencil_go4<512, OUT, 0>(H, grid, sm4, a); return;
-        default: throw FemhError{FEMH_E_ARG, "unsupported stencil block size"};
+    }
+    if constexpr (std::is_same<TIn, float>::value && std::is_same<TOut, float>::value &&
+                  std::is_same<TB, float>::value && std::is_same<TC, float>::value) {
+      if (variant == 5) {   // eligible levels have a compile-time z extent and 384-thread tiles
+        const int nt = variant_nt(lnt, maxnz, 5);
+        const size_t sm5 = stencil2b_smem_bytes(nt, nz_spec);
+        switch (nz_spec) {
+          case 16: stencil_go5<384, OUT, 16>(H, grid, sm5, a); return;
+          case 24: stencil_go5<384, OUT, 24>(H, grid, sm5, a); return;
+          case 32: stencil_go5<384, OUT, 32>(H, grid, sm5, a); return;
+          case 48: stencil_go5<384, OUT, 48>(H, grid, sm5, a); return;
+          case 64: stencil_go5<384, OUT, 64>(H, grid, sm5, a); return;
+          case 128: stencil_go5<384, OUT, 128>(H, grid, sm5, a); return;
+          default: throw FemhError{FEMH_E_ARG, "bulk-copy stencil on an ineligible level"};
+        }
       }
     }
+    if constexpr (std::is_same<T, float>::value) {
+      if (variant == 4) {
+        const int nt = variant_nt(lnt, maxnz, 4);
+        const size_t sm4 =
+            sizeof(float2) * 18 * (size_t)nt + sizeof(float) * (6 * (size_t)maxnz + 2) + 64 * sizeof(double);
+        if (nt == 384) {
+          switch (nz_spec) {
+            case 16: stencil_go4<384, OUT, 16>(H, grid, sm4, a); return;
+            case 24: stencil_go4<384, OUT, 24>(H, grid, sm4, a); return;
+            case 32: stencil_go4<384, OUT, 32>(H, grid, sm4, a); return;
+            case 48: stencil_go4<384, OUT, 48>(H, grid, sm4, a); return;
+            case 64: stencil_go4<384, OUT, 64>(H, grid, sm4, a); return;
+            case 128: stencil_go4<384, OUT, 128>(H, grid, sm4, a); return;
+            default: stencil_go4<384, OUT, 0>(H, grid, sm4, a); return;
+          }
+        }
+        if (nz_spec == 256) {
+          stencil_go4<512, OUT, 256>(H, grid, sm4, a);
+          return;
+        }
+        switch (nt) {
+          case 128: stencil_go4<128, OUT, 0>(H, grid, sm4, a); return;
+          case 256: stencil_go4<256, OUT, 0>(H, grid, sm4, a); return;
+          case 512: stencil_go4<512, OUT, 0>(H, grid, sm4, a); return;
+          default: throw FemhError{FEMH_E_ARG, "unsupported stencil block size"};
+        }
+      }
+    }
+    switch (nz_spec) {   // compile-time z extent (threads fixed per extent)
+      case 16: stencil_go<T, 512, OUT, 16>(H, grid, smem, a, variant); return;
+      case 24: stencil_go<T, 480, OUT, 24>(H, grid, smem, a, variant); return;
+      case 32: stencil_go<T, 512, OUT, 32>(H, grid, smem, a, variant); return;
+      case 48: stencil_go<T, 480, OUT, 48>(H, grid, smem, a, variant); return;
+      case 64: stencil_go<T, 512, OUT, 64>(H, grid, smem, a, variant); return;
+      case 128: stencil_go<T, 512, OUT, 128>(H, grid, smem, a, variant); return;
+      case 256: stencil_go<T, 512, OUT, 256>(H, grid, smem, a, variant); return;
+      default: break;
+    }
+    switch (lnt) {
+      case 128: stencil_go<T, 128, OUT, 0>(H, grid, smem, a, variant); break;
+      case 256: stencil_go<T, 256, OUT, 0>(H, grid, smem, a, variant); break;
+      case 512: stencil_go<T, 512, OUT, 0>(H, grid, smem, a, variant); break;
+      default: throw FemhError{FEMH_E_ARG, "unsupported stencil block size"};
+    }
+  };
+  if (!L.grouped) {
+    launch(L.nz_spec, L.NT, L.maxnz, grid, a);
+    return;
   }
-  switch (L.nz_spec) {   // compile-time z extent (threads fixed per extent)
-    case 16: stencil_go<T, 512, OUT, 16>(H, grid, smem, a, variant); return;
-    case 24: stencil_go<T, 480, OUT, 24>(H, grid, smem, a, variant); return;
-    case 32: stencil_go<T, 512, OUT, 32>(H, grid, smem, a, variant); return;
-    case 48: stencil_go<T, 480, OUT, 48>(H, grid, smem, a, variant); return;
-    case 64: stencil_go<T, 512, OUT, 64>(H, grid, smem, a, variant); return;
-    case 128: stencil_go<T, 512, OUT, 128>(H, grid, smem, a, variant); return;
-    case 256: stencil_go<T, 512, OUT, 256>(H, grid, smem, a, variant); return;
-    default: break;
-  }
-  switch (L.NT) {
-    case 128: stencil_go<T, 128, OUT, 0>(H, grid, smem, a, variant); break;
-    case 256: stencil_go<T, 256, OUT, 0>(H, grid, smem, a, variant); break;
-    case 512: stencil_go<T, 512, OUT, 0>(H, grid, smem, a, variant); break;
-    default: throw FemhError{FEMH_E_ARG, "unsupported stencil block size"};
+  // cells of several compile-time z extents: one launch per extent
+  const UnitGroups& gr = use64 ? L.g64 : (smooth_only ? L.gsmooth : L.gall);
+  for (size_t gi = 0; gi < gr.nz.size(); ++gi) {
+    StencilArgs<TIn, TOut, TB, TC> ag = a;
+    ag.units = a.units + gr.b[gi];
+    launch(gr.nz[gi], spec_nt(gr.nz[gi]), gr.nz[gi], dim3((unsigned)(gr.e[gi] - gr.b[gi]), kNumRhs), ag);
   }
 }
 
@@ -777,23 +834,27 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
         L.NT = (z0 == 24 || z0 == 48) ? 480 : 512;
       }
     }
-    {   // bulk-copy staging needs 16-byte rows and at most two row segments per tile
-      L.bulk_ok = L.nz_spec > 0 && L.nz_spec % 4 == 0 && L.nz_spec <= 128;
-      const int tr = variant_nt(L.NT, L.maxnz, 5) / std::max(1, L.maxnz);
-      for (auto& cd : L.cells) L.bulk_ok = L.bulk_ok && cd.ny >= 2 * tr + 3;
-    }
     {
-      L.bulk_ok64 = L.nz_spec > 0 && L.nz_spec % 4 == 0;
-      const int r64 = L.NT / std::max(1, L.maxnz);
-      for (auto& cd : L.cells) L.bulk_ok64 = L.bulk_ok64 && cd.ny >= r64 + 2;
+      bool all_spec = true, same = true;
+      for (auto& cd : L.cells) {
+        all_spec = all_spec && spec_nz(cd.nz);
+        same = same && cd.nz == L.cells[0].nz;
+      }
+      L.grouped = L.nz_spec == 0 && all_spec && !same;
     }
+    // bulk-copy staging needs compile-time z extents with 16-byte rows (all in
+    // the compile-time set are multiples of 4); a tile never has more rows than
+    // its cell, so each staged array takes at most three row segments (20
+    // copies per stage at most, within warp 0's lanes)
+    L.bulk_ok = (L.nz_spec > 0 || L.grouped) && L.maxnz <= 128;
+    L.bulk_ok64 = L.nz_spec > 0 || L.grouped;
     if (c.stencil_variant > 0) L.variant = c.stencil_variant;
     if (L.variant == 5 && !L.bulk_ok) L.variant = 4;
     int ss = 0, sn = 0;
     for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
       const CellDesc& cd = L.cells[ci];
       L.su_sb.push_back(ss);
-      add_stencil_units(L.all.su, ci, cd, variant_nt(L.NT, L.maxnz, L.variant), ss, 0, L.variant);
+      add_stencil_units(L.all.su, ci, cd, cell_nt(L, cd, L.variant), ss, 0, L.variant);
       L.su_se.push_back(ss);
       L.nu_sb.push_back(sn);
       add_node_units(L.all.nu, ci, (long long)cd.nx * cd.ny * cd.nz, sn);
@@ -802,8 +863,10 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
     L.level = l;
     for (auto& cd : L.cells)
       if (cd.child >= 0) L.nodes_smooth += (long long)cd.nx * cd.ny * cd.nz;
+    group_units(L, L.all.su, L.gall, true);
     for (auto& u : L.all.su)
       if (L.cells[u.cell].child >= 0) L.smooth.su.push_back(u);
+    group_units(L, L.smooth.su, L.gsmooth, false);
     for (auto& u : L.all.nu)
       if (L.cells[u.cell].child >= 0) L.smooth.nu.push_back(u);
     if (gmg)
@@ -924,6 +987,9 @@ void set_units(femh_handle* H, Level& L, const FullLists& F, const std::vector<c
   put_s(L.all.su, L.all.d_su, filt_s(F.all_su));
   put_s(L.smooth.su, L.smooth.d_su, filt_s(F.smooth_su));
   if (L.use64) put_s(L.su64, L.d_su64, filt_s(F.su64));
+  group_units(L, L.all.su, L.gall, false);   // filtering keeps the z-extent order
+  group_units(L, L.smooth.su, L.gsmooth, false);
+  if (L.use64) group_units(L, L.su64, L.g64, false);
   put_n(L.all.nu, L.all.d_nu, filt_n(F.all_nu));
   put_n(L.smooth.nu, L.smooth.d_nu, filt_n(F.smooth_nu));
 }
@@ -938,11 +1004,13 @@ void build_stencil_units(femh_handle* H, Level& L, int chunk) {
   int ss = 0;
   for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
     L.su_sb.push_back(ss);
-    add_stencil_units(L.all.su, ci, L.cells[ci], variant_nt(L.NT, L.maxnz, L.variant), ss, chunk, L.variant);
+    add_stencil_units(L.all.su, ci, L.cells[ci], cell_nt(L, L.cells[ci], L.variant), ss, chunk, L.variant);
     L.su_se.push_back(ss);
   }
+  group_units(L, L.all.su, L.gall, true);
   for (auto& u : L.all.su)
     if (L.cells[u.cell].child >= 0) L.smooth.su.push_back(u);
+  group_units(L, L.smooth.su, L.gsmooth, false);
   cudaStream_t s = H->stream;
   Arena& ar = H->setup;
   L.all.d_su = upload(ar, L.all.su, s);
@@ -961,9 +1029,10 @@ void build_stencil_units64(femh_handle* H, Level& L, int chunk, int variant) {
   int ss = 0;
   for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
     L.su64_sb.push_back(ss);
-    add_stencil_units(L.su64, ci, L.cells[ci], L.NT, ss, chunk, variant);
+    add_stencil_units(L.su64, ci, L.cells[ci], cell_nt(L, L.cells[ci], variant), ss, chunk, variant);
     L.su64_se.push_back(ss);
   }
+  group_units(L, L.su64, L.g64, true);
   cudaStream_t s = H->stream;
   Arena& ar = H->setup;
   L.d_su64 = upload(ar, L.su64, s);

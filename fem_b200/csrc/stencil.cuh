@@ -1255,7 +1255,8 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned
 // runs kBulkSlots-1 steps ahead of the one in use; no per-thread loads of
 // inputs remain.
 // Requirements (checked by the host): nz % 4 == 0 on every cell, 16-byte
-// aligned arrays, ny >= 2*TR+3 so that each array needs at most two segments.
+// aligned arrays.  A tile has at most ny rows, so an array spans at most three
+// row segments: at most 20 copies per stage, one per lane of warp 0.
 constexpr int kBulkSlots = 4;
 
 template <int NT, int OUT, int NZ>

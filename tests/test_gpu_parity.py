@@ -226,3 +226,20 @@ def test_batch_matches_single(femh):
     for r, C in zip(rhos, Cb):
         Cs, _ = femh.Engine().homogenize(r)
         assert _rel(C, Cs) < TOL_FP64
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed_pc"])
+def test_batch_of_mixed_extents_matches_single(femh, precision):
+    """Cells of several z extents with compile-time kernels in one batch: the
+    level's stencil units are grouped by extent and each group launches its
+    own kernel (here the staged ones, forced); every C^H equals that of a
+    single-cell solve."""
+    from fem_b200 import fields
+    rhos = [fields.binary_cell(n, 0.45, seed=40 + i) for i, n in enumerate((16, 32, 24, 16, 48))]
+    prec, var, tol = ((femh.FP64, 6, TOL_FP64) if precision == "fp64" else (femh.MIXED_PC, 5, TOL_MIXED))
+    Cb, infos, _ = femh.Engine(precision=prec, stencil_variant=var).batch(rhos, h=None)
+    for r, C, info in zip(rhos, Cb, infos):
+        assert info["status"] == 0
+        Cs, _ = femh.Engine(precision=prec).homogenize(r)
+        assert _rel(C, Cs) < tol
+
