@@ -1211,7 +1211,18 @@ void prepare_operator(femh_handle* H) {
       }
       {
         Prof prof_(H, "k_coarse_factor", 0.0);
-        k_coarse_factor<<<n, 256, 0, s>>>(L.d_cells, L.d_coarse_list, L.d_A, L.d_Awork, L.d_aoff, L.d_cstat);
+        if (L.coarse_maxm <= kCoarseSmemM) {   // packed triangle in shared memory
+          static bool attr = false;
+          if (!attr) {
+            CK(cudaFuncSetAttribute(k_coarse_factor_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)coarse_factor_smem_bytes(kCoarseSmemM)));
+            attr = true;
+          }
+          k_coarse_factor_smem<<<n, 1024, coarse_factor_smem_bytes(L.coarse_maxm), s>>>(
+              L.d_cells, L.d_coarse_list, L.d_A, L.d_aoff, L.d_cstat);
+        } else {
+          k_coarse_factor<<<n, 256, 0, s>>>(L.d_cells, L.d_coarse_list, L.d_A, L.d_Awork, L.d_aoff, L.d_cstat);
+        }
         LAUNCH_CHECK(H);
       }
     }

@@ -569,6 +569,74 @@ __global__ void k_coarse_factor(const CellDesc* cells, const int* list, double* 
   if (threadIdx.x == 0) status[blockIdx.x] = bad;
 }
 
+// The same factorisation and inverse for coarse systems of m <= kCoarseSmemM
+// unknowns (3 x 64 nodes): the lower triangle of A packed in shared memory
+// (row i at i(i+1)/2), right-looking Cholesky in place (one warp per trailing
+// row, lanes over its columns), then A^{-1} column by column, one warp per
+// column: forward L y = e_c from row c on (y = 0 above), backward L^T x = y,
+// each row's dot product split over the lanes.  Written over A.
+constexpr int kCoarseSmemM = 192;
+inline size_t coarse_factor_smem_bytes(int m) {
+  return sizeof(double) * ((size_t)m * (m + 1) / 2 + 32 * (size_t)m);
+}
+__global__ void __launch_bounds__(1024) k_coarse_factor_smem(const CellDesc* cells, const int* list, double* A,
+                                                             const long long* aoff, int* status) {
+  extern __shared__ double csm[];
+  const CellDesc cd = cells[list[blockIdx.x]];
+  const int m = 3 * cd.nx * cd.ny * cd.nz;
+  double* Ag = A + aoff[blockIdx.x];
+  double* Lp = csm;                               // packed lower triangle
+  double* Yw = csm + (size_t)m * (m + 1) / 2;     // [32 warps][m] column buffers
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  auto P = [](int i, int j) { return i * (i + 1) / 2 + j; };   // j <= i
+  __shared__ int bad;
+  if (tid == 0) bad = 0;
+  for (int i = warp; i < m; i += nw)
+    for (int j = lane; j <= i; j += 32) Lp[P(i, j)] = Ag[(long long)i * m + j];
+  __syncthreads();
+  for (int k = 0; k < m; ++k) {
+    if (tid == 0) {
+      const double d = Lp[P(k, k)];
+      if (!(d > 0.0) && !bad) bad = k + 1;
+      Lp[P(k, k)] = sqrt(fmax(d, 1e-300));
+    }
+    __syncthreads();
+    const double dk = Lp[P(k, k)];
+    for (int i = k + 1 + tid; i < m; i += nt) Lp[P(i, k)] /= dk;
+    __syncthreads();
+    for (int i = k + 1 + warp; i < m; i += nw) {
+      const double lik = Lp[P(i, k)];
+      for (int j = k + 1 + lane; j <= i; j += 32) Lp[P(i, j)] -= lik * Lp[P(j, k)];
+    }
+    __syncthreads();
+  }
+  double* y = Yw + (size_t)warp * m;
+  for (int c = warp; c < m; c += nw) {
+    for (int i = lane; i < c; i += 32) y[i] = 0.0;
+    __syncwarp();
+    for (int i = c; i < m; ++i) {   // forward: L y = e_c
+      double sacc = 0.0;
+      for (int j = c + lane; j < i; j += 32) sacc += Lp[P(i, j)] * y[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+      if (lane == 0) y[i] = ((i == c ? 1.0 : 0.0) - sacc) / Lp[P(i, i)];
+      __syncwarp();
+    }
+    for (int i = m - 1; i >= 0; --i) {   // backward: L^T x = y
+      double sacc = 0.0;
+      for (int j = i + 1 + lane; j < m; j += 32) sacc += Lp[P(j, i)] * y[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+      if (lane == 0) y[i] = (y[i] - sacc) / Lp[P(i, i)];
+      __syncwarp();
+    }
+    for (int i = lane; i < m; i += 32) Ag[(long long)i * m + c] = y[i];
+    __syncwarp();
+  }
+  __syncthreads();
+  if (tid == 0) status[blockIdx.x] = bad;
+}
+
 // Coarse solve e = A^{-1} b for one (cell, rhs) per CTA (A^{-1} symmetric).
 template <typename TB, typename TX>
 __global__ void k_coarse_solve(const CellDesc* cells, const int* list, const double* Ainv,
