@@ -1271,7 +1271,7 @@ void vcycle_level_down(femh_handle* H, int l, const TB* b, TM* cur, TM* oth, TM*
   if (!L.coarse_list.empty()) {
     dim3 g((unsigned)L.coarse_list.size(), kNumRhs);
     Prof prof_(H, "k_coarse_solve", 0.0);
-    k_coarse_solve<TB, TM><<<g, 256, sizeof(double) * L.coarse_maxm, s>>>(
+    k_coarse_solve<TB, TM><<<g, 1024, sizeof(double) * L.coarse_maxm, s>>>(
         L.d_cells, L.d_coarse_list, L.d_A, L.d_aoff, b, sol, stt, L.ntot);
     LAUNCH_CHECK(H);
   }

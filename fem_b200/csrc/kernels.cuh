@@ -653,11 +653,19 @@ __global__ void k_coarse_solve(const CellDesc* cells, const int* list, const dou
   }
   __syncthreads();
   const double* M = Ainv + aoff[blockIdx.x];
-  for (int t = threadIdx.x; t < m; t += blockDim.x) {
+  // one warp per row t (A^{-1} is symmetric: row t is read contiguously), the
+  // row's dot product split over the lanes and summed by shuffles
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int t = warp; t < m; t += nw) {
+    const double* Mr = M + (long long)t * m;
     double s = 0.0;
-    for (int j = 0; j < m; ++j) s += M[(long long)j * m + t] * sb[j];
-    const int n = t / 3, c = t % 3;
-    st_val(x + ((long long)rhs * 3 + c) * ntot + cd.off + n, (n == 0) ? 0.0 : s);
+    for (int j = lane; j < m; j += 32) s += Mr[j] * sb[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      const int n = t / 3, c = t % 3;
+      st_val(x + ((long long)rhs * 3 + c) * ntot + cd.off + n, (n == 0) ? 0.0 : s);
+    }
   }
 }
 
