@@ -41,12 +41,14 @@ struct ElemConst {
   double uhat0[kNumRhs][3][8]; // Hadamard transform of ue0^I(h=1)
 };
 
+// (i, j, k) of node n of a cell; n < nx*ny*nz < 2^32, so 32-bit unsigned
+// division (far cheaper than 64-bit) is exact.
 __device__ __forceinline__ void node_ijk(long long n, int ny, int nz, int& i, int& j, int& k) {
-  const long long p = (long long)ny * nz;
-  i = (int)(n / p);
-  const long long rem = n - (long long)i * p;
-  j = (int)(rem / nz);
-  k = (int)(rem - (long long)j * nz);
+  const unsigned nn = (unsigned)n, p = (unsigned)ny * (unsigned)nz;
+  const unsigned ii = nn / p, rem = nn - ii * p, jj = rem / (unsigned)nz;
+  i = (int)ii;
+  j = (int)jj;
+  k = (int)(rem - jj * (unsigned)nz);
 }
 __device__ __forceinline__ long long lin(int i, int j, int k, int ny, int nz) {
   return ((long long)i * ny + j) * nz + k;
