@@ -432,8 +432,11 @@ void add_stencil_units(std::vector<StencilUnit>& out, int cellidx, const CellDes
   }
 }
 
-void add_node_units(std::vector<NodeUnit>& out, int cellidx, long long nn, int& slot) {
-  const long long chunk = 2048;
+// Node work units of chunk nodes (even, so node pairs never straddle units).
+// Level 0 (whose CG reductions keep per-unit partial sums) uses 2048; the
+// coarser levels' node kernels are latency-bound, and smaller units give them
+// more CTAs.
+void add_node_units(std::vector<NodeUnit>& out, int cellidx, long long nn, int& slot, long long chunk) {
   for (long long b = 0; b < nn; b += chunk)
     out.push_back(NodeUnit{cellidx, slot++, b, std::min(nn, b + chunk)});
 }
@@ -857,7 +860,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
       add_stencil_units(L.all.su, ci, cd, cell_nt(L, cd, L.variant), ss, 0, L.variant);
       L.su_se.push_back(ss);
       L.nu_sb.push_back(sn);
-      add_node_units(L.all.nu, ci, (long long)cd.nx * cd.ny * cd.nz, sn);
+      add_node_units(L.all.nu, ci, (long long)cd.nx * cd.ny * cd.nz, sn, l == 0 ? 2048 : 256);
       L.nu_se.push_back(sn);
     }
     L.level = l;
@@ -1099,7 +1102,7 @@ void autotune_level0_fp64(femh_handle* H) {
 
 // Project autotuner for the stencil's tile shape: for every level whose
 // stencil runs, time the damped-Jacobi sweep (the most launched mode) for
-// x-chunk lengths {4, 8, 16, 32, 64, whole cell} on the level's own buffers
+// x-chunk lengths {1, 2, 4, 8, 16, 32, 64, whole cell} on the level's own buffers
 // and keep the fastest.  Results are cached per level signature in the handle.
 template <typename T>
 void autotune_levels(femh_handle* H, bool mg) {
@@ -1121,10 +1124,6 @@ void autotune_levels(femh_handle* H, bool mg) {
       build_stencil_units(H, L, it->second / 16);
       continue;
     }
-    if (L.ntot < 4096) {   // tiny levels: launch-bound, the heuristic is fine
-      H->tune_cache[key] = L.chunk * 16 + L.variant;
-      continue;
-    }
     T* in = (T*)(L.xa ? L.xa : H->cg_r);
     T* out = (T*)(L.xb ? L.xb : H->cg_q);
     CK(cudaMemsetAsync(L.kc, 0, sizeof(T) * L.ntot, s));
@@ -1132,9 +1131,11 @@ void autotune_levels(femh_handle* H, bool mg) {
     CK(cudaMemsetAsync(in, 0, sizeof(T) * 18 * L.ntot, s));
     int best = L.chunk, best_var = L.variant;
     float best_ms = 1e30f;
+    // short x-chunks give small, latency-bound levels more CTAs of fewer steps
     std::vector<int> cands;
-    for (int cand : {4, 8, 16, 32, 64, maxnx})
+    for (int cand : {1, 2, 4, 8, 16, 32, 64, maxnx})
       if (cand <= maxnx && std::find(cands.begin(), cands.end(), cand) == cands.end()) cands.push_back(cand);
+    const int reps = L.ntot < 65536 ? 7 : 3;   // small levels time in microseconds: more samples
     std::vector<int> vars = {1, 2};
     if (std::is_same<T, float>::value) vars = {2, 3, 4};
     if (std::is_same<T, float>::value && L.bulk_ok) vars.push_back(5);
@@ -1145,7 +1146,7 @@ void autotune_levels(femh_handle* H, bool mg) {
       L.variant = var;
       build_stencil_units(H, L, cand);
       float ms_min = 1e30f;
-      for (int rep = 0; rep < 3; ++rep) {
+      for (int rep = 0; rep < reps; ++rep) {
         CK(cudaEventRecord(H->ev0, s));
         stencil<T, OUT_JACOBI>(H, L, smooth, (const T*)in, out, (const T*)in, (const T*)L.kc, nullptr, nullptr,
                                0.5);
