@@ -146,6 +146,61 @@ HadK host_hadk(const double K[576]) {
   return h;
 }
 
+// Largest eigenvalue of diag(K0)^-1 K0, by cyclic Jacobi rotations of the
+// symmetric diag^-1/2 K0 diag^-1/2.  For K = sum_e c_e K0_e with c_e >= 0,
+// u.K u <= lambda u.D u holds element by element, so this bounds the spectrum
+// of D^-1 K for every coefficient field, on every rediscretised level (5.318
+// for nu = 0.3, the volumetric mode of one element).
+double host_jacobi_bound(const double K[576]) {
+  double S[24][24];
+  for (int i = 0; i < 24; ++i)
+    for (int j = 0; j < 24; ++j) S[i][j] = K[i * 24 + j] / std::sqrt(K[i * 24 + i] * K[j * 24 + j]);
+  for (int sweep = 0; sweep < 64; ++sweep) {
+    double off = 0.0;
+    for (int i = 0; i < 24; ++i)
+      for (int j = i + 1; j < 24; ++j) off += S[i][j] * S[i][j];
+    if (off < 1e-28) break;
+    for (int p = 0; p < 24; ++p)
+      for (int q = p + 1; q < 24; ++q) {
+        if (std::fabs(S[p][q]) < 1e-300) continue;
+        const double th = (S[q][q] - S[p][p]) / (2.0 * S[p][q]);
+        const double t = (th >= 0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < 24; ++k) {
+          const double a = S[k][p], b = S[k][q];
+          S[k][p] = c * a - s * b;
+          S[k][q] = s * a + c * b;
+        }
+        for (int k = 0; k < 24; ++k) {
+          const double a = S[p][k], b = S[q][k];
+          S[p][k] = c * a - s * b;
+          S[q][k] = s * a + c * b;
+        }
+      }
+  }
+  double m = 0.0;
+  for (int i = 0; i < 24; ++i) m = std::max(m, S[i][i]);
+  return m;
+}
+
+// Damping weights of an m-sweep smoothing pass.  ratio > 0: the reciprocal
+// roots of the degree-m Chebyshev polynomial on [lmax/ratio, lmax], smallest
+// weight first (the pass then multiplies the error by the scaled Chebyshev
+// polynomial, below 1 in magnitude on all of (0, lmax]); ratio == 0: omega for
+// every sweep.
+std::vector<double> smooth_weights(int m, double lmax, double ratio, double omega) {
+  std::vector<double> w;
+  for (int k = 1; k <= m; ++k) {
+    if (ratio > 0.0) {
+      const double a = lmax / ratio, c = 0.5 * (lmax + a), h = 0.5 * (lmax - a);
+      w.push_back(1.0 / (c + h * std::cos(M_PI * (2 * k - 1) / (2.0 * m))));
+    } else {
+      w.push_back(omega);
+    }
+  }
+  return w;
+}
+
 ElemConst host_elemconst(const double K[576]) {
   ElemConst ec{};
   for (int I = 0; I < kNumRhs; ++I) {
@@ -273,6 +328,7 @@ struct femh_handle {
   ElemConst ec{};
   ElemConst* d_ec = nullptr;
   double* d_K0 = nullptr;
+  std::vector<double> w_pre, w_post;   // damping weight of each smoothing sweep
   Arena perm;   // lives as long as the handle
 
   // setup cache
@@ -1251,7 +1307,7 @@ bool fuse_rz(const femh_handle* H) {
 // One V-cycle of the multigrid preconditioner: z = V(r0), levels in TM
 // arithmetic/storage with coefficients TMC; r0 (level-0 right-hand side) may
 // be of another type (FP64 CG residual feeding an FP32 V-cycle).  Level 0's xa
-// must already hold the first damped-Jacobi sweep omega*invd*r0 (written by
+// must already hold the first damped-Jacobi sweep w_pre[0]*invd*r0 (written by
 // the CG update kernel).  Buffer roles are fixed by the sweep counts, so the
 // launch sequence is identical every iteration (graph capture).
 // Profile name of a per-level kernel ("<base>_L<level>"), interned in the
@@ -1266,7 +1322,7 @@ template <typename TM, typename TMC, typename TB>
 void vcycle_level_down(femh_handle* H, int l, const TB* b, TM* cur, TM* oth, TM* sol) {
   const femh_config& c = H->cfg;
   cudaStream_t s = H->stream;
-  const double om = c.omega;
+  const std::vector<double>& w = H->w_pre;
   const CGState* stt = H->d_state;
   Level& L = H->levels[l];
   if (!L.coarse_list.empty()) {
@@ -1279,15 +1335,15 @@ void vcycle_level_down(femh_handle* H, int l, const TB* b, TM* cur, TM* oth, TM*
   if (L.smooth.su.empty()) return;
   if (l > 0) {
     Prof prof_(H, level_name(H, "k_jacobi0", l), 18.0 * (sizeof(TB) + sizeof(TM)) * L.nodes_smooth);
-    k_jacobi0<TB, TM><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, L.smooth.d_nu, b, cur, (TM*)nullptr, L.invd, om, stt,
+    k_jacobi0<TB, TM><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, L.smooth.d_nu, b, cur, (TM*)nullptr, L.invd, w[0], stt,
                                                           L.ntot);
     LAUNCH_CHECK(H);
   }
   for (int sw = 1; sw < c.pre_smooth; ++sw) {
-    stencil<TM, OUT_JACOBI>(H, L, true, (const TM*)cur, oth, b, (const TMC*)L.kc, nullptr, stt, om);
+    stencil<TM, OUT_JACOBI>(H, L, true, (const TM*)cur, oth, b, (const TMC*)L.kc, nullptr, stt, w[sw]);
     std::swap(cur, oth);
   }
-  stencil<TM, OUT_RESID>(H, L, true, (const TM*)cur, oth, b, (const TMC*)L.kc, nullptr, stt, om);
+  stencil<TM, OUT_RESID>(H, L, true, (const TM*)cur, oth, b, (const TMC*)L.kc, nullptr, stt, w[0]);
   Level& C = H->levels[l + 1];
   Prof prof_(H, level_name(H, "k_restrict", l), 18.0 * sizeof(TM) * (L.nodes_smooth + C.ntot));
   k_restrict<TM, TM><<<NODE_GRID(C.all), 256, 0, s>>>(L.d_cells, C.d_cells, C.all.d_nu, oth, (TM*)C.bv, stt,
@@ -1311,9 +1367,9 @@ void vcycle_level_up(femh_handle* H, int l, const TB* b, TM* x, TM* t, const TM*
   }
   for (int sw = 0; sw < c.post_smooth; ++sw) {
     if (dot_part && sw + 1 == c.post_smooth)   // last sweep also forms z . b
-      stencil<TM, OUT_JACOBI_DOT>(H, L, true, (const TM*)x, t, b, (const TMC*)L.kc, dot_part, stt, c.omega);
+      stencil<TM, OUT_JACOBI_DOT>(H, L, true, (const TM*)x, t, b, (const TMC*)L.kc, dot_part, stt, H->w_post[sw]);
     else
-      stencil<TM, OUT_JACOBI>(H, L, true, (const TM*)x, t, b, (const TMC*)L.kc, nullptr, stt, c.omega);
+      stencil<TM, OUT_JACOBI>(H, L, true, (const TM*)x, t, b, (const TMC*)L.kc, nullptr, stt, H->w_post[sw]);
     std::swap(x, t);
   }
 }
@@ -1388,7 +1444,7 @@ void pcg_iteration(femh_handle* H, const typename PR::K* kcg) {
                (18.0 * (5 * sizeof(TV) + sizeof(TP) + (gmg ? sizeof(TM) : 0) + (rm ? sizeof(TM) : 0)) + 4.0) *
                    (double)L0.ntot);
     k_cg_update<TV, TP, TV, TM><<<NODE_GRID(L0.all), 256, 0, s>>>(
-        L0.d_cells, L0.all.d_nu, x, r, p, q, L0.invd, gmg ? (TM*)L0.xa : (TM*)nullptr, rm, c.omega, stt,
+        L0.d_cells, L0.all.d_nu, x, r, p, q, L0.invd, gmg ? (TM*)L0.xa : (TM*)nullptr, rm, H->w_pre[0], stt,
         H->d_part_n, L0.ntot);
     LAUNCH_CHECK(H);
   }
@@ -1460,7 +1516,7 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
     {
       Prof prof_(H, "k_jacobi0", 0.0);
       k_jacobi0<TV, TM><<<NODE_GRID(L0.all), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, r, (TM*)L0.xa, rm,
-                                                          L0.invd, c.omega, stt, L0.ntot);
+                                                          L0.invd, H->w_pre[0], stt, L0.ntot);
       LAUNCH_CHECK(H);
     }
     const bool fuse = fuse_rz(H);
@@ -1821,6 +1877,7 @@ void check_config(const femh_config& c) {
   if (!(c.tol > 0.0) || c.max_iter < 1) throw FemhError{FEMH_E_ARG, "tol > 0 and max_iter >= 1 are required"};
   if (c.precision == FEMH_MIXED && (!(c.inner_tol > 0.0) || c.max_outer < 1))
     throw FemhError{FEMH_E_ARG, "inner_tol > 0 and max_outer >= 1 are required"};
+  if (!(c.cheb_ratio == 0.0 || c.cheb_ratio > 1.0)) throw FemhError{FEMH_E_ARG, "cheb_ratio must be 0 or > 1"};
   if (c.coarse_avg < 0 || c.coarse_avg > 2) throw FemhError{FEMH_E_ARG, "coarse_avg must be 0, 1 or 2"};
   if (!(c.E_s > 0.0) || c.E_min < 0.0 || !(c.rho_max >= c.rho_min))
     throw FemhError{FEMH_E_ARG, "bad material law parameters"};
@@ -1844,9 +1901,9 @@ femh_status femh_config_default(femh_config* c) {
   c->rho_max = 1.0;
   c->precision = FEMH_FP64;
   c->solver = FEMH_GMG_PCG;
-  c->pre_smooth = 2;
-  c->post_smooth = 2;
-  c->omega = 0.35;   // < 2 / 5.36: damped Jacobi stable for any coefficient field (nu = 0.3)
+  c->pre_smooth = 3;
+  c->post_smooth = 3;
+  c->omega = 0.35;   // < 2 / 5.32: damped Jacobi stable for any coefficient field (nu = 0.3)
   c->coarse_max_nodes = 64;
   c->tol = 1e-10;
   c->max_iter = 20000;
@@ -1858,6 +1915,7 @@ femh_status femh_config_default(femh_config* c) {
   c->autotune = 1;
   c->stencil_variant = 0;
   c->warm_start = 0;
+  c->cheb_ratio = 64.0;   // 128^3 smooth cell, mixed: 146 iterations (2+2, omega) -> 86
   return FEMH_OK;
 }
 
@@ -1878,6 +1936,12 @@ femh_status femh_create(femh_handle** out, const femh_config* cfg) {
     host_k0(cfg->nu, H->K0);
     H->hk = host_hadk(H->K0);
     H->ec = host_elemconst(H->K0);
+    {
+      const double lmax = host_jacobi_bound(H->K0);
+      H->w_pre = smooth_weights(std::max(cfg->pre_smooth, 1), lmax, cfg->cheb_ratio, cfg->omega);
+      H->w_post = smooth_weights(std::max(cfg->post_smooth, 1), lmax, cfg->cheb_ratio, cfg->omega);
+      std::reverse(H->w_post.begin(), H->w_post.end());   // the pre-smoother's factors in reverse
+    }
     H->d_ec = H->perm.arr<ElemConst>(1);
     H->d_K0 = H->perm.arr<double>(576);
     CK(cudaMemcpy(H->d_ec, &H->ec, sizeof(ElemConst), cudaMemcpyHostToDevice));

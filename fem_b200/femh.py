@@ -55,6 +55,7 @@ class _Config(ctypes.Structure):
         ("inner_tol", ctypes.c_double), ("max_outer", ctypes.c_int),
         ("store_bf16", ctypes.c_int), ("graph_chunk", ctypes.c_int), ("coarse_avg", ctypes.c_int),
         ("autotune", ctypes.c_int), ("stencil_variant", ctypes.c_int), ("warm_start", ctypes.c_int),
+        ("cheb_ratio", ctypes.c_double),
     ]
 
 
@@ -123,8 +124,8 @@ class Config:
     rho_max: float = 1.0
     precision: int = FP64
     solver: int = GMG_PCG
-    pre_smooth: int = 2
-    post_smooth: int = 2
+    pre_smooth: int = 3
+    post_smooth: int = 3
     omega: float = 0.35
     coarse_max_nodes: int = 64
     tol: float = 1e-10
@@ -137,6 +138,7 @@ class Config:
     autotune: int = 1
     stencil_variant: int = 0
     warm_start: int = 0
+    cheb_ratio: float = 64.0
 
     def to_c(self) -> _Config:
         c = _Config()

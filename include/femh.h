@@ -67,7 +67,8 @@ typedef struct {
   double rho_min, rho_max; /* clamp applied before the law (fast_fem clamps 1e-3..1) */
   int precision;          /* FEMH_FP64 | FEMH_MIXED | FEMH_MIXED_PC */
   int solver;             /* FEMH_JACOBI_PCG | FEMH_GMG_PCG */
-  int pre_smooth, post_smooth; /* damped-Jacobi sweeps per level (GMG) */
+  int pre_smooth, post_smooth; /* damped-Jacobi sweeps per level (GMG); equal counts keep the
+                                  V-cycle symmetric, which CG needs */
   double omega;           /* Jacobi damping */
   int coarse_max_nodes;   /* coarsen until a level has <= this many nodes (GMG) */
   double tol;             /* relative residual ||b - K x|| / ||b||, FP64 */
@@ -92,6 +93,11 @@ typedef struct {
                              starts from that solution (chi) instead of zero -- the
                              line-search / descent case of fast_fem/run3d.cpp:238-289;
                              results agree with a cold start within the tolerance */
+  double cheb_ratio;      /* 0: every smoothing sweep is damped by omega; > 1: the sweeps
+                             of a pass use the reciprocal roots of the Chebyshev
+                             polynomial of that degree on [lmax/cheb_ratio, lmax], lmax =
+                             the largest eigenvalue of diag(K0)^-1 K0 (a bound on the
+                             spectrum of D^-1 K for every coefficient field) */
 } femh_config;
 
 typedef struct {
@@ -111,7 +117,8 @@ typedef struct {
 
 typedef struct femh_handle femh_handle;
 
-/* Defaults: SIMP E_s=1, E_min=1e-6, p=3, nu=0.3, FP64 GMG-PCG, tol 1e-10. */
+/* Defaults: SIMP E_s=1, E_min=1e-6, p=3, nu=0.3, FP64 GMG-PCG, tol 1e-10, 3 + 3
+ * Jacobi sweeps per level with Chebyshev-root weights (cheb_ratio 64). */
 femh_status femh_config_default(femh_config* cfg);
 
 /* Create an engine on cfg->device.  Replaces ElasticHexFEM/Homogenization

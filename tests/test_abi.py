@@ -53,13 +53,14 @@ def test_config_default_matches_binding(lib):
 
 def test_bad_config_rejected_before_device_use(lib):
     from fem_b200.femh import _Config
-    c = _Config()
-    lib.femh_config_default(ctypes.byref(c))
-    c.nu = 0.7
-    h = ctypes.c_void_p()
     lib.femh_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(_Config)]
-    assert lib.femh_create(ctypes.byref(h), ctypes.byref(c)) == 1   # FEMH_E_ARG
-    assert not h.value
+    for field, value in (("nu", 0.7), ("cheb_ratio", 0.5), ("cheb_ratio", -2.0)):
+        c = _Config()
+        lib.femh_config_default(ctypes.byref(c))
+        setattr(c, field, value)
+        h = ctypes.c_void_p()
+        assert lib.femh_create(ctypes.byref(h), ctypes.byref(c)) == 1, field   # FEMH_E_ARG
+        assert not h.value
 
 
 def test_null_handle_is_an_argument_error(lib):

@@ -151,6 +151,32 @@ def test_fp64_C_matches_oracle(femh, oracle, n, solver):
     assert _rel(C, Co) < TOL_FP64
 
 
+@pytest.mark.parametrize("smoothing", [(2, 2, 3.0), (2, 2, 16.0), (3, 3, 16.0), (1, 1, 4.0)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed_pc"])
+def test_chebyshev_smoother_C_matches_oracle(femh, oracle, precision, smoothing):
+    """Chebyshev-root damping weights in the V-cycle (pre sweeps, post sweeps,
+    ratio) reach the oracle's C^H on the 32^3 binary cell: the smoother changes
+    the iteration count, not the solution."""
+    from fem_b200 import fields
+    pre, post, ratio = smoothing
+    rho = fields.binary_cell(32, 0.5, seed=1)
+    Co = _oracle_C(oracle, "binary32", rho)
+    prec = {"fp64": femh.FP64, "mixed_pc": femh.MIXED_PC}[precision]
+    e = femh.Engine(precision=prec, pre_smooth=pre, post_smooth=post, cheb_ratio=ratio)
+    C, info = e.homogenize(rho)
+    assert info["status"] == 0 and max(info["rel_residual"]) < 1e-10
+    assert _rel(C, Co) < (TOL_FP64 if precision == "fp64" else TOL_MIXED)
+
+
+_ORACLE_C = {}
+
+
+def _oracle_C(oracle, key, rho):
+    if key not in _ORACLE_C:
+        _ORACLE_C[key] = oracle.homogenize(rho)[0]
+    return _ORACLE_C[key]
+
+
 @pytest.mark.parametrize("solver", ["jacobi", "gmg"])
 @pytest.mark.parametrize("bf16", [0, 1])
 def test_mixed_C_matches_oracle(femh, oracle, solver, bf16):
