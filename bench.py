@@ -283,8 +283,8 @@ def main():
         "data": "synthetic (seeded filtered-noise densities)",
         "config": {"workload": f"{n}^3 periodic cell, smooth rho in [1e-3,1] (sigma 4), 6 load cases, "
                                f"FP64 CG + FP32 GMG V-cycle to 1e-10 + adjoint dL/drho",
-                   "grid": n, "dof": 3 * n ** 3, "rhs": 6, "solver": "GMG-PCG (damped Jacobi 2+2, "
-                   "rediscretised coarse levels, FP64 dense coarse solve)",
+                   "grid": n, "dof": 3 * n ** 3, "rhs": 6, "solver": "GMG-PCG (Jacobi 3+3 with Chebyshev-root "
+                   "weights, rediscretised coarse levels, FP64 dense coarse solve)",
                    "l2": "inputs and vectors larger than L2 (no flush needed)",
                    "parallelism": f"replicas x{world} (independent cells, one per GPU)"},
         "clocks": clk.summary(),
