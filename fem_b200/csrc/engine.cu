@@ -469,7 +469,7 @@ MatLaw make_law(const femh_config& c) {
 void add_stencil_units(std::vector<StencilUnit>& out, int cellidx, const CellDesc& cd, int NT,
                        int& slot, int chunk_req = 0, int variant = 2) {
   const int R = NT / cd.nz;
-  const bool two_rows = variant == 2 || variant == 4 || variant == 5 || variant == 7;
+  const bool two_rows = variant == 2 || variant == 4 || variant == 5;
   const int maxrows = std::max(1, std::min(two_rows ? 2 * R - 1 : R - 1, cd.ny));
   const int ntiles = (cd.ny + maxrows - 1) / maxrows;
   const int chunk = chunk_req > 0 ? std::min(chunk_req, cd.nx)
@@ -501,13 +501,9 @@ template <typename T> size_t esize() { return sizeof(T); }
 
 // Threads per CTA of a stencil variant on a level: the packed two-row kernel
 // needs up to ~160 registers a thread, so it runs 384-thread CTAs where its
-// tiles still hold at least two thread rows; variant 7 runs the staged kernel
-// in 256-thread CTAs capped at 128 registers, two per SM.  Units cut for 7
-// (at most 2*(256/nz)-1 rows) also fit the 384- and 512-thread kernels that
-// stand in for it (FP64 twin, unaligned buffers).
+// tiles still hold at least two thread rows.
 int variant_nt(int level_nt, int maxnz, int variant) {
   if ((variant == 4 || variant == 5) && level_nt > 384 && 384 >= 2 * maxnz) return 384;
-  if (variant == 7 && level_nt > 256 && 256 >= 2 * maxnz) return 256;
   return level_nt;
 }
 
@@ -633,7 +629,7 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   int variant = use64 ? L.variant64 : L.variant;
   if (!std::is_same<T, float>::value) {   // packed-FP32 kernels: FP64 twin with the same units
     if (variant == 3) variant = 1;
-    if (variant == 4 || variant == 5 || variant == 7) variant = 2;
+    if (variant == 4 || variant == 5) variant = 2;
   } else if (variant == 6) {   // the staged FP64 kernel's FP32 twin has the same units
     variant = 1;
   }
@@ -645,7 +641,7 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
     if (!(ok && L.bulk_ok64 && al(in) && al(out) && al(kc) && al(L.invd) && (!b || al(b)) && L.ntot % 4 == 0))
       variant = 1;
   }
-  if (variant == 5 || variant == 7) {   // bulk-copy staging: FP32 storage, 16-byte aligned rows, eligible level
+  if (variant == 5) {   // bulk-copy staging: FP32 storage, 16-byte aligned rows, eligible level
     const bool f32 = std::is_same<TIn, float>::value && std::is_same<TOut, float>::value &&
                      std::is_same<TB, float>::value && std::is_same<TC, float>::value;
     auto al = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
@@ -719,20 +715,9 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
     }
     if constexpr (std::is_same<TIn, float>::value && std::is_same<TOut, float>::value &&
                   std::is_same<TB, float>::value && std::is_same<TC, float>::value) {
-      if (variant == 5 || variant == 7) {   // eligible levels: compile-time z extent, 384/256-thread tiles
-        const int nt = variant_nt(lnt, maxnz, variant);
+      if (variant == 5) {   // eligible levels have a compile-time z extent and 384-thread tiles
+        const int nt = variant_nt(lnt, maxnz, 5);
         const size_t sm5 = stencil2b_smem_bytes(nt, nz_spec);
-        if (nt == 256) {
-          switch (nz_spec) {
-            case 16: stencil_go5<256, OUT, 16>(H, grid, sm5, a); return;
-            case 24: stencil_go5<256, OUT, 24>(H, grid, sm5, a); return;
-            case 32: stencil_go5<256, OUT, 32>(H, grid, sm5, a); return;
-            case 48: stencil_go5<256, OUT, 48>(H, grid, sm5, a); return;
-            case 64: stencil_go5<256, OUT, 64>(H, grid, sm5, a); return;
-            case 128: stencil_go5<256, OUT, 128>(H, grid, sm5, a); return;
-            default: throw FemhError{FEMH_E_ARG, "bulk-copy stencil on an ineligible level"};
-          }
-        }
         switch (nz_spec) {
           case 16: stencil_go5<384, OUT, 16>(H, grid, sm5, a); return;
           case 24: stencil_go5<384, OUT, 24>(H, grid, sm5, a); return;
@@ -923,7 +908,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
     L.bulk_ok = (L.nz_spec > 0 || L.grouped) && L.maxnz <= 128;
     L.bulk_ok64 = L.nz_spec > 0 || L.grouped;
     if (c.stencil_variant > 0) L.variant = c.stencil_variant;
-    if ((L.variant == 5 || L.variant == 7) && !L.bulk_ok) L.variant = 4;
+    if (L.variant == 5 && !L.bulk_ok) L.variant = 4;
     int ss = 0, sn = 0;
     for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
       const CellDesc& cd = L.cells[ci];
@@ -1209,10 +1194,7 @@ void autotune_levels(femh_handle* H, bool mg) {
     const int reps = L.ntot < 65536 ? 7 : 3;   // small levels time in microseconds: more samples
     std::vector<int> vars = {1, 2};
     if (std::is_same<T, float>::value) vars = {2, 3, 4};
-    if (std::is_same<T, float>::value && L.bulk_ok) {
-      vars.push_back(5);
-      vars.push_back(7);
-    }
+    if (std::is_same<T, float>::value && L.bulk_ok) vars.push_back(5);
     if (std::is_same<T, double>::value && L.bulk_ok64) vars.push_back(6);
     if (H->cfg.stencil_variant > 0) vars = {H->cfg.stencil_variant};
     for (int var : vars)
@@ -1895,7 +1877,7 @@ void check_config(const femh_config& c) {
   if (!(c.tol > 0.0) || c.max_iter < 1) throw FemhError{FEMH_E_ARG, "tol > 0 and max_iter >= 1 are required"};
   if (c.precision == FEMH_MIXED && (!(c.inner_tol > 0.0) || c.max_outer < 1))
     throw FemhError{FEMH_E_ARG, "inner_tol > 0 and max_outer >= 1 are required"};
-  if (c.stencil_variant < 0 || c.stencil_variant > 7) throw FemhError{FEMH_E_ARG, "stencil_variant must be 0..7"};
+  if (c.stencil_variant < 0 || c.stencil_variant > 6) throw FemhError{FEMH_E_ARG, "stencil_variant must be 0..6"};
   if (!(c.cheb_ratio == 0.0 || c.cheb_ratio > 1.0)) throw FemhError{FEMH_E_ARG, "cheb_ratio must be 0 or > 1"};
   if (c.coarse_avg < 0 || c.coarse_avg > 2) throw FemhError{FEMH_E_ARG, "coarse_avg must be 0, 1 or 2"};
   if (!(c.E_s > 0.0) || c.E_min < 0.0 || !(c.rho_max >= c.rho_min))

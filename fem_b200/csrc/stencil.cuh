@@ -1260,7 +1260,7 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned
 constexpr int kBulkSlots = 4;
 
 template <int NT, int OUT, int NZ>
-__global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))   // 256 threads: two CTAs per SM
+__global__ void __launch_bounds__(NT, 1)
 stencil2b_kernel(StencilArgs<float, float, float, float> a) {
   static_assert(NZ > 0 && NZ % 4 == 0, "staged rows need a compile-time z extent, multiple of 4");
   extern __shared__ __align__(16) unsigned char smem_raw[];
