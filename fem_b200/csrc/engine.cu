@@ -1308,7 +1308,8 @@ bool fuse_rz(const femh_handle* H) {
 // arithmetic/storage with coefficients TMC; r0 (level-0 right-hand side) may
 // be of another type (FP64 CG residual feeding an FP32 V-cycle).  Level 0's xa
 // must already hold the first damped-Jacobi sweep w_pre[0]*invd*r0 (written by
-// the CG update kernel).  Buffer roles are fixed by the sweep counts, so the
+// the CG update kernel); each coarser level's xa is written by the restriction
+// that forms its right-hand side.  Buffer roles are fixed by the sweep counts, so the
 // launch sequence is identical every iteration (graph capture).
 // Profile name of a per-level kernel ("<base>_L<level>"), interned in the
 // handle's statistics map so that the pointer stays valid.
@@ -1333,20 +1334,17 @@ void vcycle_level_down(femh_handle* H, int l, const TB* b, TM* cur, TM* oth, TM*
     LAUNCH_CHECK(H);
   }
   if (L.smooth.su.empty()) return;
-  if (l > 0) {
-    Prof prof_(H, level_name(H, "k_jacobi0", l), 18.0 * (sizeof(TB) + sizeof(TM)) * L.nodes_smooth);
-    k_jacobi0<TB, TM><<<NODE_GRID(L.smooth), 256, 0, s>>>(L.d_cells, L.smooth.d_nu, b, cur, (TM*)nullptr, L.invd, w[0], stt,
-                                                          L.ntot);
-    LAUNCH_CHECK(H);
-  }
   for (int sw = 1; sw < c.pre_smooth; ++sw) {
     stencil<TM, OUT_JACOBI>(H, L, true, (const TM*)cur, oth, b, (const TMC*)L.kc, nullptr, stt, w[sw]);
     std::swap(cur, oth);
   }
   stencil<TM, OUT_RESID>(H, L, true, (const TM*)cur, oth, b, (const TMC*)L.kc, nullptr, stt, w[0]);
   Level& C = H->levels[l + 1];
-  Prof prof_(H, level_name(H, "k_restrict", l), 18.0 * sizeof(TM) * (L.nodes_smooth + C.ntot));
-  k_restrict<TM, TM><<<NODE_GRID(C.all), 256, 0, s>>>(L.d_cells, C.d_cells, C.all.d_nu, oth, (TM*)C.bv, stt,
+  const bool c_smooth = !C.smooth.su.empty();   // also C's first sweep from a zero guess
+  Prof prof_(H, level_name(H, "k_restrict", l),
+             18.0 * sizeof(TM) * (L.nodes_smooth + C.ntot) + (c_smooth ? (18.0 * sizeof(TM) + 4.0) * C.nodes_smooth : 0.0));
+  k_restrict<TM, TM><<<NODE_GRID(C.all), 256, 0, s>>>(L.d_cells, C.d_cells, C.all.d_nu, oth, (TM*)C.bv,
+                                                      c_smooth ? (TM*)C.xa : (TM*)nullptr, C.invd, w[0], stt,
                                                       L.ntot, C.ntot);
   LAUNCH_CHECK(H);
 }

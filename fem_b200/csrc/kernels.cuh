@@ -380,13 +380,19 @@ __global__ void k_fin_beta(CGState* stt, const int* slot_begin, const int* slot_
 // ---------------------------------------------------------- multigrid ---
 // Full-weighting restriction (transpose of trilinear prolongation):
 // bc(I) = sum_{d in {-1,0,1}^3} prod_s (1 - |d_s|/2) rf(2I + d); 0 at node 0.
+// xc != nullptr: also the coarse level's first damped-Jacobi sweep from a zero
+// guess, xc = omega * invdc * bc (as stored), on the coarse cells that are
+// smoothed there (child >= 0; the others are solved directly).
 template <typename TF, typename TCo>
 __global__ void k_restrict(const CellDesc* fine, const CellDesc* coarse, const NodeUnit* units,
-                           const TF* __restrict__ rf, TCo* __restrict__ bc, const CGState* stt, long long ntf, long long ntc) {
+                           const TF* __restrict__ rf, TCo* __restrict__ bc, TCo* __restrict__ xc,
+                           const float* __restrict__ invdc, double omega, const CGState* stt, long long ntf,
+                           long long ntc) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cc = coarse[u.cell], cf = fine[cc.parent];
   if (stt && !stt[cc.id * kNumRhs + rhs].active) return;
+  const bool smooth = xc != nullptr && cc.child >= 0;
   #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
     int i, j, k;
@@ -410,8 +416,15 @@ __global__ void k_restrict(const CellDesc* fine, const CellDesc* coarse, const N
         }
       }
     }
+    const long long g = cc.off + n;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) st_val(bc + ((long long)rhs * 3 + c) * ntc + cc.off + n, acc[c]);
+    for (int c = 0; c < 3; ++c) st_val(bc + ((long long)rhs * 3 + c) * ntc + g, acc[c]);
+    if (smooth) {
+      const double id = (double)invdc[g];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        st_val(xc + ((long long)rhs * 3 + c) * ntc + g, omega * id * (double)static_cast<TCo>(acc[c]));
+    }
   }
 }
 
