@@ -43,13 +43,8 @@ struct FemhError {
 
 // ------------------------------------------------------------ host math ---
 // K0 of a unit cube (E = 1, h = 1), 2x2x2 Gauss, local node a = 4ax+2ay+az.
-void host_k0(double nu, double K[576]) {
-  const double lam = nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = 1.0 / (2.0 * (1.0 + nu));
-  double D[6][6] = {};
-  for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b) D[a][b] = lam;
-  for (int a = 0; a < 3; ++a) D[a][a] += 2 * mu;
-  D[3][3] = D[4][4] = D[5][5] = mu;
+// Element matrix of the engineering-Voigt material matrix D (xx,yy,zz,yz,xz,xy).
+void host_k0_voigt(const double D[6][6], double K[576]) {
   std::fill(K, K + 576, 0.0);
   const double g = 1.0 / std::sqrt(3.0);
   for (int q = 0; q < 8; ++q) {
@@ -82,6 +77,36 @@ void host_k0(double nu, double K[576]) {
         K[p * 24 + r] += 0.125 * acc;
       }
   }
+}
+
+// Isotropic material matrix, E = 1.
+void iso_voigt(double nu, double D[6][6]) {
+  const double lam = nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = 1.0 / (2.0 * (1.0 + nu));
+  for (int a = 0; a < 6; ++a)
+    for (int b = 0; b < 6; ++b) D[a][b] = 0.0;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) D[a][b] = lam;
+  for (int a = 0; a < 3; ++a) D[a][a] += 2 * mu;
+  D[3][3] = D[4][4] = D[5][5] = mu;
+}
+
+void host_k0(double nu, double K[576]) {
+  double D[6][6];
+  iso_voigt(nu, D);
+  host_k0_voigt(D, K);
+}
+
+// Element matrix of femlib's force-driven coarse tensor: that tensor
+// (meshUtil::computeCoarsenedElasticityTensor, femlib/src/MeshUtilities.cpp:960-1060)
+// contracts tensor-shear strains (eps_yz, not 2 eps_yz) with the engineering
+// matrix StrainLin::EMatrix (femlib/src/StrainLin.cpp:39-58), i.e. its energy
+// is that of the matrix S D S, S = diag(1, 1, 1, 1/2, 1/2, 1/2), on
+// engineering strains -- a cubic material with the shear modulus divided by 4.
+void host_k0_force(double nu, double K[576]) {
+  double D[6][6];
+  iso_voigt(nu, D);
+  for (int a = 3; a < 6; ++a) D[a][a] *= 0.25;
+  host_k0_voigt(D, K);
 }
 
 inline double chi_k(int k, int a) {  // Hadamard character
@@ -325,6 +350,7 @@ struct femh_handle {
   long long launches = 0;
   double K0[576];
   HadK hk{};
+  HadK hk_force{};   // Hadamard factors of host_k0_force (femh_force_tensors)
   ElemConst ec{};
   ElemConst* d_ec = nullptr;
   double* d_K0 = nullptr;
@@ -1770,7 +1796,9 @@ void solve_all(femh_handle* H, std::vector<femh_solve_info>& infos) {
   }
 }
 
-void energy_C(femh_handle* H, std::vector<double>& C, std::vector<double>& dens) {
+// Energy pairs of the resident fields: C^H with the element matrix's Hadamard
+// factors k = H->hk; other factors give other bilinear forms on the same fields.
+void energy_C(femh_handle* H, std::vector<double>& C, std::vector<double>& dens, const HadK* k = nullptr) {
   Level& L0 = H->levels[0];
   cudaStream_t s = H->stream;
   EnergyArgs a{};
@@ -1782,7 +1810,7 @@ void energy_C(femh_handle* H, std::vector<double>& C, std::vector<double>& dens)
   a.ec = H->d_ec;
   a.part = H->d_part_e;
   a.ntot = L0.ntot;
-  a.k = H->hk;
+  a.k = k ? *k : H->hk;
   a.law = make_law(H->cfg);
   {
     Prof prof_(H, "k_energy", 0.0);
@@ -1934,6 +1962,11 @@ femh_status femh_create(femh_handle** out, const femh_config* cfg) {
     CK(cudaEventCreate(&H->ev1));
     host_k0(cfg->nu, H->K0);
     H->hk = host_hadk(H->K0);
+    {
+      double Kf[576];
+      host_k0_force(cfg->nu, Kf);
+      H->hk_force = host_hadk(Kf);
+    }
     H->ec = host_elemconst(H->K0);
     {
       const double lmax = host_jacobi_bound(H->K0);
@@ -2073,6 +2106,29 @@ femh_status femh_homogenize_grad(femh_handle* H, const double dLdC[36], double* 
       LAUNCH_CHECK(H);
     }
     to_host_or_dev(H, dLdrho, H->d_out, H->nvox, out_on_device);
+  });
+}
+
+femh_status femh_force_tensors(femh_handle* H, double* C_out) {
+  if (!H) return FEMH_E_ARG;
+  return guard(H, [&] {
+    if (!H->solved) throw FemhError{FEMH_E_STATE, "call femh_homogenize or femh_homogenize_batch first"};
+    if (!C_out) throw FemhError{FEMH_E_ARG, "C_out must not be NULL"};
+    // femlib's shear loads put f/2 on faces of different areas when the cell
+    // is not cubic: out of moment balance, the rotation multipliers then load
+    // the cell in the interior and its fields leave the periodic + affine space
+    for (const CellDesc& cd : H->levels[0].cells)
+      if (cd.nx != cd.ny || cd.ny != cd.nz)
+        throw FemhError{FEMH_E_ARG, "the force-driven tensor needs cubic cells (nx = ny = nz)"};
+    CK(cudaSetDevice(H->device));
+    std::vector<double> W, dens;
+    energy_C(H, W, dens, &H->hk_force);
+    // unit tensor-shear coarse strains instead of unit engineering ones: the
+    // shear rows and columns scale by 2 (coarseGv = S, inverted, :1000-1060)
+    const double sc[6] = {1, 1, 1, 2, 2, 2};
+    for (int c = 0; c < H->ncells; ++c)
+      for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) C_out[36 * c + 6 * i + j] = sc[i] * sc[j] * W[36 * c + 6 * i + j];
   });
 }
 

@@ -30,7 +30,7 @@ JACOBI_PCG, GMG_PCG = 0, 1
 #: every exported symbol of include/femh.h
 EXPORTS = (
     "femh_config_default", "femh_create", "femh_destroy", "femh_homogenize", "femh_homogenize_grad",
-    "femh_dCdrho", "femh_full_field", "femh_fluctuation", "femh_apply_operator", "femh_homogenize_batch",
+    "femh_dCdrho", "femh_force_tensors", "femh_full_field", "femh_fluctuation", "femh_apply_operator", "femh_homogenize_batch",
     "femh_last_error", "femh_set_stream", "femh_kernel_launches", "femh_profile", "femh_profile_read",
     "femh_energy_noalloc",
 )
@@ -94,6 +94,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.femh_homogenize.argtypes = [vp, ip, ip, ip, ctypes.c_double, vp, ip, dp, ctypes.POINTER(_Info)]
     L.femh_homogenize_grad.argtypes = [vp, dp, vp, ip]
     L.femh_dCdrho.argtypes = [vp, vp, ip]
+    L.femh_force_tensors.argtypes = [vp, vp]
     L.femh_full_field.argtypes = [vp, ip, vp, ip]
     L.femh_fluctuation.argtypes = [vp, vp, ip]
     L.femh_apply_operator.argtypes = [vp, ip, ip, ip, ctypes.c_double, vp, vp, vp, ip]
@@ -175,6 +176,7 @@ class Engine:
             raise FemhError(st, "femh_create failed (no CUDA device or bad config)")
         self.h = h
         self.shape = None
+        self._ncells = 0   # cells of the last solve (their fields stay resident)
 
     def close(self):
         if getattr(self, "h", None):
@@ -235,6 +237,7 @@ class Engine:
         allow = (FEMH_OK, FEMH_E_NOT_CONVERGED, FEMH_E_BREAKDOWN) if allow_unconverged else (FEMH_OK,)
         self._check(st, allow)
         self.shape = (nx, ny, nz)
+        self._ncells = 1
         return C, _info_dict(info)
 
     def grad(self, dLdC, out=None):
@@ -252,6 +255,15 @@ class Engine:
             out = np.zeros((21,) + tuple(self.shape))
         self._check(self.lib.femh_dCdrho(self.h, _ptr(out), _is_dev(out)))
         return out
+
+    def force_tensors(self):
+        """femlib's force-driven coarse tensor (femh_force_tensors) of each
+        cell of the last solve: [6, 6] after homogenize, [n, 6, 6] after batch."""
+        if self._ncells < 1:
+            raise FemhError(6, "call homogenize or batch first")
+        out = np.zeros((self._ncells, 6, 6))
+        self._check(self.lib.femh_force_tensors(self.h, _ptr(out)))
+        return out[0] if self.shape is not None else out
 
     def full_field(self, load_case: int):
         nx, ny, nz = self.shape
@@ -274,6 +286,7 @@ class Engine:
         h = 1.0 / nx if h is None else float(h)
         self._check(self.lib.femh_apply_operator(self.h, nx, ny, nz, h, _ptr(rho), _ptr(u), _ptr(y), 0))
         self.shape = None
+        self._ncells = 0
         return y
 
     def batch(self, rhos: Sequence[np.ndarray], h: float | None = None, dLdC=None, allow_unconverged=False):
@@ -299,6 +312,8 @@ class Engine:
                                             dp, gp, infos)
         allow = (FEMH_OK, FEMH_E_NOT_CONVERGED, FEMH_E_BREAKDOWN) if allow_unconverged else (FEMH_OK,)
         self._check(st, allow)
+        self.shape = None
+        self._ncells = n
         grads = None
         if g is not None:
             grads, o = [], 0

@@ -267,6 +267,135 @@ void NumericalCoarseningUsingMultigrid::computeBatch(const std::vector<std::vect
   if (nc) lastInfo = infos.back();
 }
 
+// ---------------------------------------------------------- NumericalCoarsening
+namespace {
+// Inverse of a nonsingular 6x6 matrix (Gauss-Jordan with partial pivoting).
+bool invert6(const double A[36], double Ai[36]) {
+  double M[6][12];
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) {
+      M[i][j] = A[6 * i + j];
+      M[i][6 + j] = i == j ? 1.0 : 0.0;
+    }
+  for (int c = 0; c < 6; ++c) {
+    int p = c;
+    for (int r = c + 1; r < 6; ++r)
+      if (std::fabs(M[r][c]) > std::fabs(M[p][c])) p = r;
+    if (!(std::fabs(M[p][c]) > 0.0)) return false;
+    if (p != c)
+      for (int j = 0; j < 12; ++j) std::swap(M[p][j], M[c][j]);
+    const double inv = 1.0 / M[c][c];
+    for (int j = 0; j < 12; ++j) M[c][j] *= inv;
+    for (int r = 0; r < 6; ++r) {
+      if (r == c || M[r][c] == 0.0) continue;
+      const double f = M[r][c];
+      for (int j = 0; j < 12; ++j) M[r][j] -= f * M[c][j];
+    }
+  }
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) Ai[6 * i + j] = M[i][6 + j];
+  return true;
+}
+}  // namespace
+
+NumericalCoarsening::~NumericalCoarsening() {
+  if (h_) femh_destroy(h_);
+}
+
+void NumericalCoarsening::init(int N[3], int iNbBlockRep, int iNbSubdiv, const std::vector<BaseMaterial>& mats) {
+  if (mats.size() != 2) throw Error(FEMH_E_ARG, "two base materials are required (the engine's two-material law)");
+  m_nbBlockRep = iNbBlockRep;
+  m_nbSubdiv = iNbSubdiv;
+  m_E.assign(2, 0.0);
+  double nu[2];
+  for (int i = 0; i < 2; ++i) fromLamesParametersToYoungModulusPoissonRatio(mats[i].lambda, mats[i].mu, m_E[i], nu[i]);
+  if (!(m_E[0] > 0.0 && m_E[1] > 0.0)) throw Error(FEMH_E_ARG, "base materials need a positive stiffness");
+  if (std::fabs(nu[0] - nu[1]) > 1e-12) throw Error(FEMH_E_ARG, "base materials must share one Poisson ratio");
+  if (h_) femh_destroy(h_);
+  h_ = nullptr;
+  femh_config c;
+  femh_config_default(&c);
+  c.interp = FEMH_INTERP_BINARY;   // material index 1 -> bin_hi, 0 -> bin_lo
+  c.bin_hi = m_E[1];
+  c.bin_lo = m_E[0];
+  c.nu = nu[1];
+  check(nullptr, femh_create(&h_, &c));
+  (void)N;
+}
+
+void NumericalCoarsening::rho_of(const std::vector<int>& cells, std::vector<double>& rho) const {
+  rho.resize(cells.size());
+  for (size_t i = 0; i < cells.size(); ++i) {
+    if (cells[i] != 0 && cells[i] != 1) throw Error(FEMH_E_ARG, "material indices must be 0 or 1");
+    rho[i] = cells[i] == 1 ? 1.0 : 0.0;
+  }
+}
+
+void NumericalCoarsening::append(const double CH[36], const double Cf[36], const int n[3],
+                                 const std::vector<int>& mats, const std::vector<double>& dens, StructureType t,
+                                 std::vector<double>& tv, std::vector<double>& pv) const {
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j <= i; ++j) tv.push_back(Cf[i * 6 + j]);
+  double r = 0.0;   // computeMaterialDensity (Utilities/src/cfgMaterialUtilities.cpp:660-671)
+  for (int m : mats) r += dens.at(m);
+  r /= (double)mats.size();
+  double S[36];   // compliance: the coarse strain under a macro stress sigma is S sigma
+  if (!invert6(CH, S)) throw Error(FEMH_E_ARG, "C^H is singular");
+  const double dx = 1.0 / std::max(n[0], std::max(n[1], n[2]));   // ElementRegGrid: longest side 1
+  const double area[3] = {n[1] * n[2] * dx * dx, n[0] * n[2] * dx * dx, n[0] * n[1] * dx * dx};
+  const int naxis = t == Cubic ? 1 : 3;
+  pv.push_back(r);
+  for (int a = 0; a < naxis; ++a) pv.push_back(area[a] / S[7 * a]);   // f / eps_aa, eps_aa = S_aa f / A_a
+  pv.push_back(-S[6 * 1 + 0] / S[0]);                                 // nu_xy = -eps_yy / eps_xx (x load)
+  if (t != Cubic) {
+    pv.push_back(-S[6 * 2 + 0] / S[0]);   // nu_xz (x load)
+    pv.push_back(-S[6 * 2 + 1] / S[7]);   // nu_yz (y load)
+  }
+  for (int i = 0; i < naxis; ++i) pv.push_back(Cf[(3 + i) * 6 + 3 + i]);
+}
+
+void NumericalCoarsening::computeCoarsenedElasticityTensorAndParameters3D(
+    const std::vector<int>& iMaterials, int N[3], const std::vector<double>& iDens, StructureType t,
+    std::vector<double>& tv, std::vector<double>& pv) {
+  if (!h_) throw Error(FEMH_E_STATE, "init() first");
+  std::vector<int> cells;
+  repMaterialAssignment(N[0], N[1], N[2], iMaterials, m_nbBlockRep, m_nbBlockRep, m_nbBlockRep, m_nbSubdiv, cells);
+  const int n[3] = {N[0] * m_nbBlockRep * m_nbSubdiv, N[1] * m_nbBlockRep * m_nbSubdiv,
+                    N[2] * m_nbBlockRep * m_nbSubdiv};
+  std::vector<double> rho;
+  rho_of(cells, rho);
+  double CH[36], Cf[36];
+  const double dx = 1.0 / std::max(n[0], std::max(n[1], n[2]));
+  check(h_, femh_homogenize(h_, n[0], n[1], n[2], dx, rho.data(), 0, CH, &lastInfo), true);
+  check(h_, femh_force_tensors(h_, Cf));
+  append(CH, Cf, n, iMaterials, iDens, t, tv, pv);
+}
+
+void NumericalCoarsening::computeBatch(const std::vector<std::vector<int>>& iMaterials, int N[3],
+                                       const std::vector<double>& iDens, StructureType t,
+                                       std::vector<double>& tv, std::vector<double>& pv) {
+  if (!h_) throw Error(FEMH_E_STATE, "init() first");
+  const size_t nc = iMaterials.size();
+  if (nc == 0) return;
+  const int n[3] = {N[0] * m_nbBlockRep * m_nbSubdiv, N[1] * m_nbBlockRep * m_nbSubdiv,
+                    N[2] * m_nbBlockRep * m_nbSubdiv};
+  const double dx = 1.0 / std::max(n[0], std::max(n[1], n[2]));
+  std::vector<std::vector<double>> rho(nc);
+  std::vector<femh_cell> cells(nc);
+  for (size_t c = 0; c < nc; ++c) {
+    std::vector<int> m;
+    repMaterialAssignment(N[0], N[1], N[2], iMaterials[c], m_nbBlockRep, m_nbBlockRep, m_nbBlockRep, m_nbSubdiv, m);
+    rho_of(m, rho[c]);
+    cells[c] = femh_cell{n[0], n[1], n[2], dx, rho[c].data()};
+  }
+  std::vector<double> CH(36 * nc), Cf(36 * nc);
+  std::vector<femh_solve_info> infos(nc);
+  check(h_, femh_homogenize_batch(h_, (int)nc, cells.data(), CH.data(), nullptr, nullptr, infos.data()), true);
+  check(h_, femh_force_tensors(h_, Cf.data()));
+  for (size_t c = 0; c < nc; ++c) append(&CH[36 * c], &Cf[36 * c], n, iMaterials[c], iDens, t, tv, pv);
+  lastInfo = infos.back();
+}
+
 // ------------------------------------------------------------ binary files
 template <class T>
 bool writeBinary(const std::string& file, const std::vector<T>& v) {

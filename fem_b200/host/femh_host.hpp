@@ -147,6 +147,55 @@ class NumericalCoarseningUsingMultigrid {
               StructureType t, std::vector<double>& tv, std::vector<double>& pv);
 };
 
+// femlib's force-driven coarsening, NumericalCoarsening
+// (SamplesGenerator/NumericalCoarsening.h:20-90, .cpp:116-133, 266-340): the
+// same init / computeCoarsenedElasticityTensorAndParameters3D calls and
+// outputs.  The reference applies unit face forces, solves the multiplier
+// system with PARDISO and reads C and the parameters off the harmonic
+// displacements; here one strain-driven solve gives C^H and the fields, and
+// femh_force_tensors evaluates femlib's tensor formula on them.  Appends the
+// 21 lower-triangle entries of that tensor and (rho, Y, nu_xy, G) for Cubic,
+// (rho, Yx, Yy, Yz, nu_xy, nu_xz, nu_yz, G_yz, G_xz, G_xy) otherwise, with
+// Y_a = f / eps_aa and nu_ab = -eps_bb / eps_aa of the coarse strains eps =
+// (C^H)^-1 sigma under the unit face force f on faces of area A_a (sigma_aa =
+// f / A_a; the mesh spans 1 along its longest side) and G_i = C(3+i, 3+i).
+// Cells must be cubic (n = N * rep * subdiv equal on all axes; femh_force_tensors).
+// Every base material must have the same Poisson ratio (the engine scales one
+// element matrix per voxel) and a positive stiffness (femlib's fixing of
+// isolated vertices of a zero-stiffness void is not needed then).  femlib also
+// scales the diagonal of K by 1 + 1e-5; these are the exact values, from which
+// femlib's outputs differ at about that level.
+class NumericalCoarsening {
+ public:
+  enum StructureType { General, Cubic, Orthotropic };
+
+  NumericalCoarsening() = default;
+  ~NumericalCoarsening();
+  NumericalCoarsening(const NumericalCoarsening&) = delete;
+  NumericalCoarsening& operator=(const NumericalCoarsening&) = delete;
+
+  void init(int N[3], int iNbBlockRep, int iNbSubdiv, const std::vector<BaseMaterial>& iBaseMaterials);
+  void computeCoarsenedElasticityTensorAndParameters3D(const std::vector<int>& iMaterials, int N[3],
+                                                       const std::vector<double>& iBaseMaterialDensities,
+                                                       StructureType iType, std::vector<double>& ioTensorValues,
+                                                       std::vector<double>& ioParameters);
+  // Many structures in one engine call.
+  void computeBatch(const std::vector<std::vector<int>>& iMaterials, int N[3],
+                    const std::vector<double>& iBaseMaterialDensities, StructureType iType,
+                    std::vector<double>& ioTensorValues, std::vector<double>& ioParameters);
+
+  femh_solve_info lastInfo{};
+
+ private:
+  femh_handle* h_ = nullptr;
+  int m_nbBlockRep = 1, m_nbSubdiv = 1;
+  std::vector<double> m_E;   // Young's modulus of each base material
+  void rho_of(const std::vector<int>& cells, std::vector<double>& rho) const;
+  void append(const double CH[36], const double Cf[36], const int n[3], const std::vector<int>& mats,
+              const std::vector<double>& dens, StructureType t, std::vector<double>& tv,
+              std::vector<double>& pv) const;
+};
+
 // cfgMaterialUtilities::repMaterialAssignment (Utilities/src/cfgMaterialUtilities.cpp:914-956)
 void repMaterialAssignment(int nx, int ny, int nz, const std::vector<int>& iMaterialCombIndices, int repX,
                            int repY, int repZ, int iNbSubdivisions, std::vector<int>& oMaterials);

@@ -144,6 +144,29 @@ femh_status femh_homogenize_grad(femh_handle* h, const double dLdC[36], double* 
 /* dC^H_IJ/drho_e for the 21 lower-triangle pairs, layout [21][nx*ny*nz]. */
 femh_status femh_dCdrho(femh_handle* h, double* out, int out_on_device);
 
+/* femlib's force-driven coarse tensor of every cell of the last solve
+ * (femh_homogenize: 1 cell; femh_homogenize_batch: ncell cells), C_out
+ * [cell][36] row major.  NumericalCoarsening::computeCoarsenedElasticityTensor-
+ * AndParameters3D (SamplesGenerator/NumericalCoarsening.cpp:262-340) solves
+ * six face-force load cases with periodic-jump, translation and rotation
+ * multipliers (femlib/src/EMeshStiffness.cpp:52-274) and forms
+ * C = G^-T (sum_e sum_q w_q Gv^T E Gv / nelem) G^-1 from the coarse and local
+ * strains of those fields (femlib/src/MeshUtilities.cpp:960-1060).  Its fields
+ * span the same space as the six strain-driven fluctuation fields solved here,
+ * and the formula does not depend on the basis, so this evaluates it on those
+ * fields: femlib's Voigt columns hold tensor shear strains against the
+ * engineering matrix E, hence C = S W' S with S = diag(1,1,1,2,2,2) and W' the
+ * energy pairs of the material E with its shear modulus divided by 4.
+ * Cubic cells only (FEMH_E_ARG otherwise): on an nx != ny cell femlib's shear
+ * loads (f/2 on faces of different areas) are out of moment balance and its
+ * rotation multipliers load the interior, so its fields leave that space.
+ * femlib additionally scales the diagonal of K by 1 + 1e-5
+ * (NumericalCoarsening.cpp:1262-1264); this is the exact (unregularised)
+ * value, which femlib's differs from at that 1e-5 level.  Equals C^H only for
+ * homogeneous cells.  (E, nu) of the reference's parameters come from the
+ * compliance (C^H)^-1 under its unit face loads, see femh_host.hpp. */
+femh_status femh_force_tensors(femh_handle* h, double* C_out);
+
 /* Full-cell displacement of load case I on (nx+1)(ny+1)(nz+1) nodes, layout
  * [node][3] with node (i*(ny+1)+j)*(nz+1)+k, including the affine jump on the
  * + faces: fast_fem/FEM3DFun.cpp:31-56 copyPeriodicU. */

@@ -4,7 +4,9 @@
 //      central-difference check of df (fast_fem/run3d.cpp:291-323 check_df);
 //   2. NumericalCoarseningUsingMultigrid init + computeCoarsened... on a
 //      replicated/subdivided structure (21 tensor values + 4 parameters), and
-//      the batched call against the one-at-a-time call;
+//      the batched call against the one-at-a-time call; the same for femlib's
+//      force-driven NumericalCoarsening (Cubic and General parameters, a
+//      non-cubic cell rejected);
 //   3. level*.bin round trip (cfgUtil::writeBinary / readBinary format).
 // Prints one JSON object; tests/test_gpu_host.py checks it (also against the
 // oracle).  Exit code != 0 on a failed in-program check.
@@ -110,6 +112,37 @@ int main() {
     for (int j = 0; j < 4; ++j)
       for (int k = 0; k < 4; ++k) mat0.push_back(structs[0][(i * 4 + j) * 4 + k]);
   print_vec("struct0", mat0);
+  // ------------------------------------------------------------- 2b
+  // femlib's force-driven NumericalCoarsening on the same structures and
+  // materials (both base materials have nu = 0.3)
+  NumericalCoarsening fc;
+  fc.init(N, 1, 2, mats);
+  std::vector<double> ftv, fpv, ftvb, fpvb;
+  for (auto& s : structs)
+    fc.computeCoarsenedElasticityTensorAndParameters3D(s, N, dens, NumericalCoarsening::Cubic, ftv, fpv);
+  fc.computeBatch(structs, N, dens, NumericalCoarsening::Cubic, ftvb, fpvb);
+  double fmax = 0;
+  for (size_t i = 0; i < ftv.size(); ++i) fmax = std::fmax(fmax, std::fabs(ftv[i] - ftvb[i]));
+  for (size_t i = 0; i < fpv.size(); ++i) fmax = std::fmax(fmax, std::fabs(fpv[i] - fpvb[i]));
+  if (ftv.size() != 63 || fpv.size() != 12 || fpvb.size() != 12 || fmax > 1e-9) ++fails;
+  std::vector<double> gtv, gpv;   // General: three Y, three nu, three G
+  fc.computeCoarsenedElasticityTensorAndParameters3D(structs[0], N, dens, NumericalCoarsening::General, gtv, gpv);
+  if (gpv.size() != 10) ++fails;
+  bool rejected = false;   // a non-cubic cell is an argument error
+  try {
+    int M[3] = {4, 4, 2};
+    std::vector<int> flat(32, 1);
+    std::vector<double> t2, p2;
+    fc.computeCoarsenedElasticityTensorAndParameters3D(flat, M, dens, NumericalCoarsening::Cubic, t2, p2);
+  } catch (const Error& e) {
+    rejected = e.code == FEMH_E_ARG;
+  }
+  if (!rejected) ++fails;
+  print_vec("force_tensors", ftv);
+  print_vec("force_params", fpv);
+  print_vec("force_params_general", gpv);
+  std::printf("\"force_batch_max_diff\": %.3g,\n", fmax);
+  std::printf("\"force_noncubic_rejected\": %s,\n", rejected ? "true" : "false");
   // ---------------------------------------------------------------- 3
   const std::string tmp = "/tmp/femh_level0_elasticityTensors.bin";
   std::vector<float> tf(tv.begin(), tv.end()), back;

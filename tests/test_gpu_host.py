@@ -61,6 +61,31 @@ def test_coarsening_outputs(host_out, oracle):
     assert G == pytest.approx(Co[3, 3], rel=1e-8)
 
 
+def test_force_driven_coarsening_outputs(host_out, oracle):
+    """femh_host::NumericalCoarsening (femlib's force-driven class) against the
+    oracle's restatement of femlib's multiplier system on structure 0 (8^3 after
+    subdivision): the 21 tensor values and (rho, Y, nu_xy, G) within the FP64
+    bar; the batched call equals the one-at-a-time call; General gives three
+    Y, three nu, three G; a non-cubic cell is rejected."""
+    from oracle import femlib_force as ff
+    tv = np.array(host_out["force_tensors"])
+    pv = np.array(host_out["force_params"])
+    assert tv.size == 63 and pv.size == 12 and host_out["force_batch_max_diff"] < 1e-9
+    assert host_out["force_noncubic_rejected"]
+    s0 = np.array(host_out["struct0"]).reshape(4, 4, 4)
+    cells = np.repeat(np.repeat(np.repeat(s0, 2, 0), 2, 1), 2, 2).astype(int)
+    lame = [(0.1, 0.15), (1.0 / 2.6, 0.3 / (1.3 * 0.4))]
+    E = [mu * (3 * lam + 2 * mu) / (lam + mu) for mu, lam in lame]
+    nu = lame[1][1] / (2 * (lame[1][1] + lame[1][0]))
+    C, lower, params = ff.coarsen(cells.ravel(), (8, 8, 8), E, nu, mats_in=s0.ravel().astype(int),
+                                  regularize=False)
+    assert np.abs(tv[:21] - lower).max() < 1e-8 * np.abs(lower).max()
+    assert np.abs(pv[:4] - params).max() < 1e-8 * np.abs(params).max()
+    _, _, pg = ff.coarsen(cells.ravel(), (8, 8, 8), E, nu, mats_in=s0.ravel().astype(int), cubic=False,
+                          regularize=False)
+    assert np.abs(np.array(host_out["force_params_general"]) - pg).max() < 1e-8 * np.abs(pg).max()
+
+
 def test_binary_roundtrip(host_out):
     assert host_out["binary_roundtrip"] and host_out["fails"] == 0
 

@@ -126,3 +126,64 @@ def test_k0_matches_reference_femlib_code(oracle):
         K = np.zeros((24, 24))
         assert L.femlib_k0(ctypes.c_double(1.0), ctypes.c_double(nu), K.ctypes.data_as(ctypes.c_void_p)) == 0
         assert np.abs(K - oracle.k0(1.0, nu, 1.0)).max() < 2e-8
+
+
+# ---------------------------------------------------------------- femlib's force-driven coarsening
+E2, NU2 = (0.26, 1.0), 0.3
+
+
+def _binary(n, seed):
+    return (np.random.default_rng(seed).random(n) < 0.5).astype(int).ravel()
+
+
+def test_femlib_force_homogeneous_is_isotropic():
+    """Face-force loading of a uniform cubic cell returns the material itself:
+    C = E(nu), Y = E, nu_xy = nu, G = mu (without the 1e-5 diagonal scaling
+    exactly; with it within that scaling)."""
+    from oracle import femlib_force as ff
+    mats = np.ones(27, int)
+    iso = ff.iso_matrix(1.0, NU2)
+    for reg, tol in ((False, 1e-12), (True, 1e-4)):
+        C, tv, pv = ff.coarsen(mats, (3, 3, 3), E2, NU2, regularize=reg)
+        assert np.abs(C - iso).max() < tol
+        assert np.allclose(pv, [1.0, 1.0, NU2, iso[3, 3]], rtol=tol, atol=0)
+        assert tv.size == 21
+
+
+@pytest.mark.parametrize("n", [4, 5])
+def test_femlib_force_tensor_equals_strain_driven_route(n):
+    """On a cubic binary cell femlib's multiplier system (face forces, periodic
+    jumps, fixed mean translation and rotation) gives the same tensor as S W' S
+    evaluated on the six strain-driven fluctuation fields -- the route the
+    engine takes -- and its coarse strains are (C^H)^-1 sigma, so Y and nu
+    follow from the compliance."""
+    from oracle import femlib_force as ff, oracle as O
+    mats = _binary((n, n, n), seed=n)
+    us, X, nn = ff.harmonic_displacements(mats, (n, n, n), E2, NU2, regularize=False)
+    C = ff.femlib_tensor(us, X, nn, mats, E2, NU2)
+    Cf = ff.tensor_from_fields(mats, (n, n, n), E2, NU2)
+    assert np.abs(C - Cf).max() < 1e-10 * np.abs(Cf).max()
+    assert np.abs(C - C.T).max() < 1e-12 * np.abs(C).max()
+    rho = (mats.reshape(n, n, n) == 1).astype(float)
+    mat = O.material(interp=O.INTERP_BINARY, nu=NU2, bin_hi=E2[1], bin_lo=E2[0])
+    CH = O.homogenize(rho, h=1.0 / n, mat=mat, tol=1e-13, max_iter=200000)[0]
+    S = np.linalg.inv(CH)
+    for a in range(3):   # unit stress on the unit cube's faces
+        eps = ff._voigt_t(ff.coarse_strain(us[a], X, nn))
+        assert np.abs(eps[:3] - S[:3, a]).max() < 1e-10 * abs(S[a, a])
+    # femlib's shear convention makes C differ from C^H once the cell is not uniform
+    assert np.abs(C - CH).max() > 1e-3 * np.abs(CH).max()
+    # the 1e-5 diagonal scaling moves the tensor by about that much
+    Cr = ff.femlib_tensor(*ff.harmonic_displacements(mats, (n, n, n), E2, NU2, regularize=True), mats, E2, NU2)
+    assert np.abs(Cr - C).max() < 1e-4 * np.abs(C).max()
+
+
+def test_femlib_force_noncubic_shear_loads_unbalanced():
+    """Why the engine's force-driven tensor is defined for cubic cells only: on
+    a uniform 4x6x8 cell femlib's shear face loads (f/2 on faces of different
+    areas) are out of moment balance, the rotation multipliers load the
+    interior, and the tensor is no longer the material's."""
+    from oracle import femlib_force as ff
+    n = (4, 6, 8)
+    C, _, _ = ff.coarsen(np.ones(4 * 6 * 8, int), n, E2, NU2, regularize=False)
+    assert np.abs(C - ff.iso_matrix(1.0, NU2)).max() > 1e-3
