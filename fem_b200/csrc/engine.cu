@@ -42,8 +42,8 @@ struct FemhError {
   } while (0)
 
 // ------------------------------------------------------------ host math ---
-// K0 of a unit cube (E = 1, h = 1), 2x2x2 Gauss, local node a = 4ax+2ay+az.
-// Element matrix of the engineering-Voigt material matrix D (xx,yy,zz,yz,xz,xy).
+// Element matrix of a unit cube (h = 1) for the engineering-Voigt material
+// matrix D (xx,yy,zz,yz,xz,xy), 2x2x2 Gauss, local node a = 4ax+2ay+az.
 void host_k0_voigt(const double D[6][6], double K[576]) {
   std::fill(K, K + 576, 0.0);
   const double g = 1.0 / std::sqrt(3.0);
