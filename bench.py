@@ -291,13 +291,17 @@ def main():
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": gpu_launches,
         "solve": {"outer_iterations": info["outer_iterations"], "inner_iterations": info["iterations"],
-                  "rel_residual": max(info["rel_residual"])},
+                  "rel_residual": max(info["rel_residual"]),
+                  # 3 n^3 DOF times the six load cases' CG iterations, per second of
+                  # the step (rank 0's counts times the ranks)
+                  "dof_iterations_per_s": world * 3 * n ** 3 * sum(info["iterations"]) / (ms_step / 1e3)},
         "mixed_defect_correction": {"ms_per_step": msdc, "value": world / (msdc / 1e3),
                                     "outer_iterations": infodc["outer_iterations"],
                                     "inner_iterations": infodc["iterations"],
                                     "C_rel_err_vs_fp64": float(np.abs(Cdc - C64).max() / np.abs(C64).max())},
         "fp64_plain": {"ms_per_step": ms64, "value": world / (ms64 / 1e3),
                        "iterations": info64["iterations"], "mixed_speedup": ms64 / ms_step,
+                       "dof_iterations_per_s": world * 3 * n ** 3 * sum(info64["iterations"]) / (ms64 / 1e3),
                        "C_rel_err_mixed_vs_fp64": rel_err},
         "roofline": {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
