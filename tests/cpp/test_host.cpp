@@ -25,7 +25,8 @@ static void print_vec(const char* key, const std::vector<double>& v, bool last =
   std::printf("]%s\n", last ? "" : ",");
 }
 
-int main() {
+int main(int argc, char** argv) {
+  const std::string dir = argc > 1 ? argv[1] : ".";   // where the level file round trip writes
   int fails = 0;
   std::printf("{\n");
   // ---------------------------------------------------------------- 1
@@ -144,7 +145,7 @@ int main() {
   std::printf("\"force_batch_max_diff\": %.3g,\n", fmax);
   std::printf("\"force_noncubic_rejected\": %s,\n", rejected ? "true" : "false");
   // ---------------------------------------------------------------- 3
-  const std::string tmp = "/tmp/femh_level0_elasticityTensors.bin";
+  const std::string tmp = dir + "/femh_level0_elasticityTensors.bin";
   std::vector<float> tf(tv.begin(), tv.end()), back;
   std::vector<std::vector<int>> back2;
   bool ok = writeBinary(tmp, tf) && readBinary(tmp, back) && back == tf;

@@ -15,11 +15,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 @pytest.fixture(scope="module")
 def host_out(femh, tmp_path_factory):
-    exe = str(tmp_path_factory.mktemp("cpp") / "test_host")
+    work = tmp_path_factory.mktemp("cpp")
+    exe = str(work / "test_host")
     lib = os.path.join(ROOT, "fem_b200")
     subprocess.run(["g++", "-std=c++17", "-O1", "-o", exe, os.path.join(ROOT, "tests", "cpp", "test_host.cpp"),
                     f"-L{lib}", "-lfemh", f"-Wl,-rpath,{lib}"], check=True)
-    res = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    res = subprocess.run([exe, str(work)], capture_output=True, text=True, timeout=600)
     assert res.returncode == 0, res.stdout + res.stderr
     return json.loads(res.stdout)
 
