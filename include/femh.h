@@ -149,7 +149,7 @@ femh_status femh_dCdrho(femh_handle* h, double* out, int out_on_device);
  * [cell][36] row major.  NumericalCoarsening::computeCoarsenedElasticityTensor-
  * AndParameters3D (SamplesGenerator/NumericalCoarsening.cpp:262-340) solves
  * six face-force load cases with periodic-jump, translation and rotation
- * multipliers (femlib/src/EMeshStiffness.cpp:52-274) and forms
+ * multipliers (femlib/src/EMeshStiffness.cpp:53-274) and forms
  * C = G^-T (sum_e sum_q w_q Gv^T E Gv / nelem) G^-1 from the coarse and local
  * strains of those fields (femlib/src/MeshUtilities.cpp:960-1060).  Its fields
  * span the same space as the six strain-driven fluctuation fields solved here,
