@@ -289,8 +289,33 @@ class Engine:
         self._ncells = 0
         return y
 
-    def batch(self, rhos: Sequence[np.ndarray], h: float | None = None, dLdC=None, allow_unconverged=False):
-        """Many cells in one set of launches.  Returns (C [n,6,6], infos, dLdrho list or None)."""
+    def batch(self, rhos: Sequence[np.ndarray], h: float | None = None, dLdC=None, allow_unconverged=False,
+              max_nodes: int | None = None):
+        """Many cells in one set of launches.  Returns (C [n,6,6], infos, dLdrho list or None).
+
+        max_nodes: split the cells into consecutive calls of at most that many
+        voxels each (at least one cell per call); the engine keeps about 1.1 KB
+        per voxel in the mixed mode, so a call that does not fit the GPU's
+        memory fails with FEMH_E_OOM.  After a split call force_tensors() is
+        not available (the engine holds only the last part's fields)."""
+        if max_nodes is not None and sum(int(np.prod(r.shape)) for r in rhos) > max_nodes:
+            dl = None if dLdC is None else np.ascontiguousarray(dLdC, dtype=np.float64).reshape(len(rhos), 6, 6)
+            Cs, infos, grads = [], [], ([] if dLdC is not None else None)
+            i = 0
+            while i < len(rhos):
+                j, nodes = i, 0
+                while j < len(rhos) and (j == i or nodes + int(np.prod(rhos[j].shape)) <= max_nodes):
+                    nodes += int(np.prod(rhos[j].shape))
+                    j += 1
+                C, inf, g = self.batch(rhos[i:j], h=h, dLdC=None if dl is None else dl[i:j],
+                                       allow_unconverged=allow_unconverged)
+                Cs.append(C)
+                infos += inf
+                if grads is not None:
+                    grads += g
+                i = j
+            self._ncells = 0
+            return np.concatenate(Cs), infos, grads
         n = len(rhos)
         rhos = [np.ascontiguousarray(r, dtype=np.float64) for r in rhos]
         cells = (_Cell * n)()

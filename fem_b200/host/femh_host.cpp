@@ -18,6 +18,12 @@ void check(femh_handle* h, int st, bool allow_unconverged = false) {
   else std::snprintf(buf, sizeof buf, "engine creation failed (no CUDA device or bad config)");
   throw Error(st, "femh error " + std::to_string(st) + ": " + buf);
 }
+
+// Structures of n[0] x n[1] x n[2] voxels per batched engine call, at least one.
+size_t batch_cells_per_call(const int n[3], long long max_nodes) {
+  const long long cell = (long long)n[0] * n[1] * n[2];
+  return (size_t)std::max(1LL, max_nodes / std::max(1LL, cell));
+}
 }  // namespace
 
 // ---------------------------------------------------------- PiecewiseConstant3D
@@ -251,24 +257,30 @@ void NumericalCoarseningUsingMultigrid::computeBatch(const std::vector<std::vect
   if (nc == 0) return;
   const int n[3] = {N[0] * m_nbBlockRep * m_nbSubdiv, N[1] * m_nbBlockRep * m_nbSubdiv,
                     N[2] * m_nbBlockRep * m_nbSubdiv};
-  std::vector<std::vector<double>> rho(nc);
-  std::vector<femh_cell> cells(nc);
-  for (size_t c = 0; c < nc; ++c) {
-    std::vector<int> m;
-    repMaterialAssignment(N[0], N[1], N[2], iMaterials[c], m_nbBlockRep, m_nbBlockRep, m_nbBlockRep, m_nbSubdiv, m);
-    rho[c].resize(m.size());
-    for (size_t i = 0; i < m.size(); ++i) rho[c][i] = m[i] == 1 ? 1.0 : 0.0;
-    cells[c] = femh_cell{n[0], n[1], n[2], 1.0 / n[0], rho[c].data()};
+  const size_t per = batch_cells_per_call(n, maxNodesPerCall);
+  for (size_t c0 = 0; c0 < nc; c0 += per) {
+    const size_t m = std::min(per, nc - c0);
+    std::vector<std::vector<double>> rho(m);
+    std::vector<femh_cell> cells(m);
+    for (size_t c = 0; c < m; ++c) {
+      std::vector<int> mm;
+      repMaterialAssignment(N[0], N[1], N[2], iMaterials[c0 + c], m_nbBlockRep, m_nbBlockRep, m_nbBlockRep,
+                            m_nbSubdiv, mm);
+      rho[c].resize(mm.size());
+      for (size_t i = 0; i < mm.size(); ++i) rho[c][i] = mm[i] == 1 ? 1.0 : 0.0;
+      cells[c] = femh_cell{n[0], n[1], n[2], 1.0 / n[0], rho[c].data()};
+    }
+    std::vector<double> C(36 * m);
+    std::vector<femh_solve_info> infos(m);
+    check(h_, femh_homogenize_batch(h_, (int)m, cells.data(), C.data(), nullptr, nullptr, infos.data()), true);
+    for (size_t c = 0; c < m; ++c) append(&C[36 * c], iMaterials[c0 + c], iDens, t, tv, pv);
+    lastInfo = infos.back();
   }
-  std::vector<double> C(36 * nc);
-  std::vector<femh_solve_info> infos(nc);
-  check(h_, femh_homogenize_batch(h_, (int)nc, cells.data(), C.data(), nullptr, nullptr, infos.data()), true);
-  for (size_t c = 0; c < nc; ++c) append(&C[36 * c], iMaterials[c], iDens, t, tv, pv);
-  if (nc) lastInfo = infos.back();
 }
 
 // ---------------------------------------------------------- NumericalCoarsening
 namespace {
+
 // Inverse of a nonsingular 6x6 matrix (Gauss-Jordan with partial pivoting).
 bool invert6(const double A[36], double Ai[36]) {
   double M[6][12];
@@ -380,20 +392,25 @@ void NumericalCoarsening::computeBatch(const std::vector<std::vector<int>>& iMat
   const int n[3] = {N[0] * m_nbBlockRep * m_nbSubdiv, N[1] * m_nbBlockRep * m_nbSubdiv,
                     N[2] * m_nbBlockRep * m_nbSubdiv};
   const double dx = 1.0 / std::max(n[0], std::max(n[1], n[2]));
-  std::vector<std::vector<double>> rho(nc);
-  std::vector<femh_cell> cells(nc);
-  for (size_t c = 0; c < nc; ++c) {
-    std::vector<int> m;
-    repMaterialAssignment(N[0], N[1], N[2], iMaterials[c], m_nbBlockRep, m_nbBlockRep, m_nbBlockRep, m_nbSubdiv, m);
-    rho_of(m, rho[c]);
-    cells[c] = femh_cell{n[0], n[1], n[2], dx, rho[c].data()};
+  const size_t per = batch_cells_per_call(n, maxNodesPerCall);
+  for (size_t c0 = 0; c0 < nc; c0 += per) {
+    const size_t m = std::min(per, nc - c0);
+    std::vector<std::vector<double>> rho(m);
+    std::vector<femh_cell> cells(m);
+    for (size_t c = 0; c < m; ++c) {
+      std::vector<int> mm;
+      repMaterialAssignment(N[0], N[1], N[2], iMaterials[c0 + c], m_nbBlockRep, m_nbBlockRep, m_nbBlockRep,
+                            m_nbSubdiv, mm);
+      rho_of(mm, rho[c]);
+      cells[c] = femh_cell{n[0], n[1], n[2], dx, rho[c].data()};
+    }
+    std::vector<double> CH(36 * m), Cf(36 * m);
+    std::vector<femh_solve_info> infos(m);
+    check(h_, femh_homogenize_batch(h_, (int)m, cells.data(), CH.data(), nullptr, nullptr, infos.data()), true);
+    check(h_, femh_force_tensors(h_, Cf.data()));
+    for (size_t c = 0; c < m; ++c) append(&CH[36 * c], &Cf[36 * c], n, iMaterials[c0 + c], iDens, t, tv, pv);
+    lastInfo = infos.back();
   }
-  std::vector<double> CH(36 * nc), Cf(36 * nc);
-  std::vector<femh_solve_info> infos(nc);
-  check(h_, femh_homogenize_batch(h_, (int)nc, cells.data(), CH.data(), nullptr, nullptr, infos.data()), true);
-  check(h_, femh_force_tensors(h_, Cf.data()));
-  for (size_t c = 0; c < nc; ++c) append(&CH[36 * c], &Cf[36 * c], n, iMaterials[c], iDens, t, tv, pv);
-  lastInfo = infos.back();
 }
 
 // ------------------------------------------------------------ binary files

@@ -130,12 +130,15 @@ class NumericalCoarseningUsingMultigrid {
                                                        const std::vector<double>& iBaseMaterialDensities,
                                                        StructureType iType, std::vector<double>& ioTensorValues,
                                                        std::vector<double>& ioParameters);
-  // Many structures in one engine call (the sample generator's batch).
+  // Many structures in batched engine calls (the sample generator's batch),
+  // split so that one call holds at most maxNodesPerCall voxels (the engine
+  // keeps about 1.1 KB per voxel in the mixed mode: 64M voxels ~ 70 GB).
   void computeBatch(const std::vector<std::vector<int>>& iMaterials, int N[3],
                     const std::vector<double>& iBaseMaterialDensities, StructureType iType,
                     std::vector<double>& ioTensorValues, std::vector<double>& ioParameters);
 
   femh_solve_info lastInfo{};
+  long long maxNodesPerCall = 64LL << 20;
 
  private:
   femh_handle* h_ = nullptr;
@@ -179,12 +182,13 @@ class NumericalCoarsening {
                                                        const std::vector<double>& iBaseMaterialDensities,
                                                        StructureType iType, std::vector<double>& ioTensorValues,
                                                        std::vector<double>& ioParameters);
-  // Many structures in one engine call.
+  // Many structures in batched engine calls of at most maxNodesPerCall voxels.
   void computeBatch(const std::vector<std::vector<int>>& iMaterials, int N[3],
                     const std::vector<double>& iBaseMaterialDensities, StructureType iType,
                     std::vector<double>& ioTensorValues, std::vector<double>& ioParameters);
 
   femh_solve_info lastInfo{};
+  long long maxNodesPerCall = 64LL << 20;
 
  private:
   femh_handle* h_ = nullptr;

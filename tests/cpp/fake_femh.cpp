@@ -22,6 +22,8 @@ struct femh_handle {
   int nvox = 0;
 };
 
+int g_batch_calls = 0;   // femh_homogenize_batch calls so far (read by the test driver)
+
 namespace {
 void fake_C(const femh_config& c, int nx, int ny, int nz, const double* rho, double C[36]) {
   const long long n = (long long)nx * ny * nz;
@@ -85,6 +87,7 @@ femh_status femh_homogenize(femh_handle* h, int nx, int ny, int nz, double, cons
 femh_status femh_homogenize_batch(femh_handle* h, int ncell, const femh_cell* cells, double* C_out,
                                   const double*, double*, femh_solve_info* infos) {
   if (!h || ncell < 1 || !cells || !C_out) return FEMH_E_ARG;
+  ++g_batch_calls;
   h->C.clear();
   h->cubic.clear();
   for (int i = 0; i < ncell; ++i) {

@@ -12,6 +12,8 @@
 
 using namespace femh_host;
 
+extern int g_batch_calls;   // tests/cpp/fake_femh.cpp
+
 static void print_vec(const char* key, const std::vector<double>& v) {
   std::printf("\"%s\": [", key);
   for (size_t i = 0; i < v.size(); ++i) std::printf("%s%.17g", i ? ", " : "", v[i]);
@@ -47,6 +49,15 @@ int main() {
   print_vec("force_tensors_batch", tvb);
   print_vec("force_params_batch", pvb);
   print_vec("force_params_general", pvg);
+  {   // split into calls of one 4^3 structure each: same outputs, one call per structure
+    std::vector<double> ts, ps;
+    fc.maxNodesPerCall = 64;
+    const int before = g_batch_calls;
+    fc.computeBatch(structs, N, dens, NumericalCoarsening::Cubic, ts, ps);
+    std::printf("\"force_split_calls\": %d,\n", g_batch_calls - before);
+    std::printf("\"force_split_equal\": %s,\n", (ts == tvb && ps == pvb) ? "true" : "false");
+    fc.maxNodesPerCall = 64LL << 20;
+  }
   std::vector<double> cell0;   // structure 0 after repMaterialAssignment
   {
     std::vector<int> m;
@@ -84,6 +95,15 @@ int main() {
                                                      mtv, mpv);
   print_vec("mg_tensors", mtv);
   print_vec("mg_params", mpv);
+  {
+    std::vector<double> t1, p1, t2, p2;
+    mg.computeBatch(structs, N, dens, NumericalCoarseningUsingMultigrid::Cubic, t1, p1);
+    mg.maxNodesPerCall = 128;   // two 4^3 structures per call
+    const int before = g_batch_calls;
+    mg.computeBatch(structs, N, dens, NumericalCoarseningUsingMultigrid::Cubic, t2, p2);
+    std::printf("\"mg_split_calls\": %d,\n", g_batch_calls - before);
+    std::printf("\"mg_split_equal\": %s,\n", (t1 == t2 && p1 == p2) ? "true" : "false");
+  }
   // FEM3DFun objective and chain rule through a piecewise-constant field
   const int n = 4;
   PiecewiseConstant3D field;

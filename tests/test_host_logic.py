@@ -80,6 +80,14 @@ def test_force_driven_class(out):
     assert np.array_equal(np.array(out["cell0"]).reshape(4, 4, 4), cell0)
 
 
+def test_batches_split_by_node_budget(out):
+    """computeBatch splits the structures into engine calls of at most
+    maxNodesPerCall voxels (the engine's memory is about 1.1 KB per voxel) and
+    returns the same values as one call."""
+    assert out["force_split_calls"] == 3 and out["force_split_equal"]
+    assert out["mg_split_calls"] == 2 and out["mg_split_equal"]
+
+
 def test_force_driven_argument_errors(out):
     assert out["err_noncubic"] == 1        # FEMH_E_ARG from femh_force_tensors
     assert out["err_material_index"] == 1  # indices other than 0 / 1
