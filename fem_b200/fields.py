@@ -50,11 +50,13 @@ BATCH_SIZES = (16, 24, 32, 48, 64)
 BATCH_PROBS = (0.30, 0.25, 0.25, 0.15, 0.05)
 
 
-def uneven_batch(ncell: int = 4096, seed: int = 7):
+def uneven_batch(ncell: int = 4096, seed: int = 7, count: int | None = None):
+    """The seeded uneven set; ``count`` returns only its first cells (the same
+    draws as the full set)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     ns = rng.choice(BATCH_SIZES, size=ncell, p=BATCH_PROBS)
     vf = rng.uniform(0.2, 0.6, size=ncell)
     cells = []
-    for n, v in zip(ns, vf):
+    for n, v in list(zip(ns, vf))[:ncell if count is None else count]:
         cells.append((rng.random((n, n, n)) < v).astype(np.float64))
     return cells

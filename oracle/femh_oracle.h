@@ -34,6 +34,14 @@ int fo_homogenize(int nx, int ny, int nz, double h, const double* rho, const fo_
                   double rel[6]);
 int fo_num_threads(void);
 
+/* femh_oracle_mg.c: the same problem solved by geometric-multigrid PCG
+ * (returns 0 converged, 1 max_iter reached, 2 breakdown, < 0 set-up error) */
+int fo_mg_homogenize(int nx, int ny, int nz, double h, const double* rho, const fo_material* m,
+                     double tol, int max_iter, int pre, int post, double cheb_ratio, int coarse_max,
+                     double C[36], double* chi_out, int iters[6], double rel[6]);
+void fo_mg_apply(int nx, int ny, int nz, double h, const double* coef, double nu, const double* u,
+                 double* y);
+
 #ifdef __cplusplus
 }
 #endif

@@ -38,8 +38,8 @@ def material(interp=INTERP_SIMP, E_s=1.0, E_min=1e-6, penal=3.0, nu=0.3, bin_hi=
 
 def build(force: bool = False) -> str:
     """Compile the oracle with its Makefile (gcc + OpenMP)."""
-    src = os.path.join(_HERE, "femh_oracle.c")
-    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+    srcs = [os.path.join(_HERE, f) for f in ("femh_oracle.c", "femh_oracle_mg.c", "femh_oracle.h", "Makefile")]
+    if force or not os.path.exists(_LIB_PATH) or any(os.path.getmtime(_LIB_PATH) < os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-C", _HERE, "-s"], check=True)
     return _LIB_PATH
 
@@ -68,6 +68,11 @@ def lib():
         L.fo_num_threads.restype = ctypes.c_int
         L.fo_pcg1.argtypes = [ctypes.c_int] * 3 + [dp, dp, dp, dp, dp, ctypes.c_double, ctypes.c_int, dp]
         L.fo_pcg1.restype = ctypes.c_int
+        L.fo_mg_homogenize.argtypes = [ctypes.c_int] * 3 + [
+            ctypes.c_double, dp, ctypes.POINTER(Material), ctypes.c_double, ctypes.c_int, ctypes.c_int,
+            ctypes.c_int, ctypes.c_double, ctypes.c_int, dp, dp, ctypes.POINTER(ctypes.c_int), dp]
+        L.fo_mg_homogenize.restype = ctypes.c_int
+        L.fo_mg_apply.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double, dp, ctypes.c_double, dp, dp]
         _lib = L
     return _lib
 
@@ -122,6 +127,37 @@ def homogenize(rho: np.ndarray, h: float | None = None, mat: Material | None = N
     st = lib().fo_homogenize(nx, ny, nz, h, _p(rho), ctypes.byref(mat), tol, max_iter,
                              _p(C), _p(chi), iters, _p(rel))
     return C, chi, list(iters), rel, st
+
+
+def mg_homogenize(rho: np.ndarray, h: float | None = None, mat: Material | None = None,
+                  tol: float = 1e-10, max_iter: int = 2000, pre: int = 3, post: int = 3,
+                  cheb_ratio: float = 64.0, coarse_max: int = 64, want_chi: bool = True):
+    """Same problem and outputs as ``homogenize``, solved by the multigrid PCG of
+    femh_oracle_mg.c.  Returns (C[6,6], chi[6,nx,ny,nz,3] or None, iters[6],
+    rel[6], status)."""
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    nx, ny, nz = rho.shape
+    if h is None:
+        h = 1.0 / nx
+    if mat is None:
+        mat = material()
+    C = np.zeros((6, 6))
+    chi = np.zeros((6, nx, ny, nz, 3)) if want_chi else None
+    iters = (ctypes.c_int * 6)()
+    rel = np.zeros(6)
+    st = lib().fo_mg_homogenize(nx, ny, nz, h, _p(rho), ctypes.byref(mat), tol, max_iter, pre, post,
+                                cheb_ratio, coarse_max, _p(C), _p(chi) if want_chi else None, iters, _p(rel))
+    return C, chi, list(iters), rel, st
+
+
+def mg_apply(shape, c: np.ndarray, u: np.ndarray, h: float = 1.0, nu: float = 0.3) -> np.ndarray:
+    """y = K(c) u (six load cases, [6, nx, ny, nz, 3]) through the multigrid
+    file's Hadamard-form apply; the rows of node 0 come back 0 (pinned)."""
+    nx, ny, nz = shape
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    y = np.zeros_like(u)
+    lib().fo_mg_apply(nx, ny, nz, h, _p(np.ascontiguousarray(c, dtype=np.float64)), nu, _p(u), _p(y))
+    return y
 
 
 def energy(rho, chi, h=None, mat=None) -> np.ndarray:

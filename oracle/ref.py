@@ -1,0 +1,59 @@
+"""ctypes access to the reference's own code built by oracle/build_ref.sh into
+oracle/_ref/ (TEST INFRASTRUCTURE ONLY; tests/ alone import this module).
+
+* ``nc_coarsen``: SamplesGenerator's NumericalCoarsening::
+  computeCoarsenedElasticityTensorAndParameters3D
+  (SamplesGenerator/NumericalCoarsening.cpp:266-340), float as the reference
+  ships it, PARDISO replaced by Eigen's sparse LU (oracle/ref_shim/pardiso_eigen.cpp).
+* ``fastfem``: fast_fem's FEM3DFun setParam / f / df
+  (fast_fem/FEM3DFun.cpp:128-268) over a PiecewiseConstant3D field, with the
+  stand-in topoOptLib headers of oracle/ref_shim/ (its solve is the oracle's).
+
+Each returns None when the library is absent (reference tree not present at
+build time), so that the tests skip.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_REF = os.path.join(_HERE, "_ref")
+_libs: dict = {}
+
+GENERAL, CUBIC, ORTHOTROPIC = 0, 1, 2
+
+
+def _load(name):
+    if name not in _libs:
+        path = os.path.join(_REF, name)
+        _libs[name] = ctypes.CDLL(path) if os.path.exists(path) else None
+    return _libs[name]
+
+
+def available(name: str) -> bool:
+    return _load(name) is not None
+
+
+def nc_coarsen(materials: np.ndarray, E, nu, densities, stype: int = CUBIC):
+    """Reference outputs for one structure: (21 appended tensor values,
+    appended parameters).  materials: int array [nx, ny, nz]."""
+    L = _load("libnc_ref.so")
+    if L is None:
+        return None
+    dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    L.ref_nc_coarsen3d.argtypes = [ctypes.c_int] * 3 + [ip, ctypes.c_int, dp, dp, dp, ctypes.c_int, dp, dp]
+    L.ref_nc_coarsen3d.restype = ctypes.c_int
+    nx, ny, nz = materials.shape
+    m = np.ascontiguousarray(materials.ravel(), dtype=np.int32)
+    E = np.ascontiguousarray(E, dtype=np.float64)
+    nuv = np.ascontiguousarray(np.broadcast_to(np.asarray(nu, dtype=np.float64), E.shape))
+    d = np.ascontiguousarray(densities, dtype=np.float64)
+    tv, pv = np.zeros(21), np.zeros(16)
+    k = L.ref_nc_coarsen3d(nx, ny, nz, m.ctypes.data_as(ip), len(E), E.ctypes.data_as(dp), nuv.ctypes.data_as(dp),
+                           d.ctypes.data_as(dp), stype, tv.ctypes.data_as(dp), pv.ctypes.data_as(dp))
+    if k < 0:
+        raise RuntimeError(f"ref_nc_coarsen3d failed ({k})")
+    return tv, pv[:k]
