@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
@@ -257,17 +258,22 @@ ElemConst host_elemconst(const double K[576]) {
 // ------------------------------------------------------------- device mem ---
 struct Arena {
   std::vector<void*> ptrs;
+  size_t held = 0;            // bytes allocated
+  size_t limit = SIZE_MAX;    // FEMH_ARENA_LIMIT_BYTES (tests only): fail like a full device beyond it
   void* get(size_t bytes) {
     if (bytes == 0) bytes = 16;
+    if (bytes > limit - held) throw FemhError{FEMH_E_OOM, "device memory limit of this handle reached"};
     void* p = nullptr;
     CK(cudaMalloc(&p, bytes));
     ptrs.push_back(p);
+    held += bytes;
     return p;
   }
   template <typename T> T* arr(size_t n) { return static_cast<T*>(get(n * sizeof(T))); }
   void release() {
     for (void* p : ptrs) cudaFree(p);
     ptrs.clear();
+    held = 0;
   }
   ~Arena() { release(); }
 };
@@ -388,14 +394,17 @@ struct femh_handle {
   double* d_part_e = nullptr;   // energy partials [slots][21]
   double* d_C = nullptr;        // [ncells][36]
   double* d_W = nullptr;        // [ncells][21]
-  double* d_out = nullptr;      // gradient / dCdrho output [21][nvox]
+  double* d_stage = nullptr;    // output staging (dCdrho, fields, apply), allocated on first use
+  size_t stage_n = 0;           // doubles in d_stage
   double* d_nrm = nullptr;      // [ncells][6]
   bool solved = false;
   bool have_x = false;   // x64 holds the last solution of these cells (warm starts)
   std::vector<double> C_last;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  int* d_err = nullptr;   // set by a stencil kernel whose bounded wait ran out
+  int wait_limit = kWaitLimit;   // try_wait rounds of the staged kernels' stage waits
+  int* d_err = nullptr;   // [0] set by a stencil kernel whose bounded wait ran out,
+                          // [1] by k_coef on a NaN, infinite or negative density
 
   // measurement: per-kernel-class CUDA-event timing (femh_profile), and the
   // count of kernel executions including CUDA-graph replays
@@ -688,6 +697,7 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   a.k = H->hk;
   a.omega = omega;
   a.err = H->d_err;
+  a.wait_limit = H->wait_limit;
   {
     const HadK& k = H->hk;
     const double kv[8] = {k.A, k.Bd - k.Bo, k.Bo, k.D1 - k.O1, k.O1, k.D2 - k.O2, k.O2, k.G};
@@ -827,6 +837,75 @@ template <typename T>
 void autotune_levels(femh_handle* H, bool mg);
 void autotune_level0_fp64(femh_handle* H);
 
+// Device staging for outputs that the solver's own buffers cannot hold (the
+// 21 x nvox dC/drho table, full fields, layouts): allocated on first use and
+// kept until the cell set changes, so a batch that never asks for them never
+// pays their memory (21 x 8 B per voxel for dC/drho).
+void release_stage(femh_handle* H) {
+  if (H->d_stage) cudaFree(H->d_stage);
+  H->d_stage = nullptr;
+  H->stage_n = 0;
+}
+
+double* stage(femh_handle* H, size_t n) {
+  if (H->stage_n < n) {
+    release_stage(H);
+    CK(cudaMalloc(&H->d_stage, n * sizeof(double)));
+    H->stage_n = n;
+  }
+  return H->d_stage;
+}
+
+// Where a gradient is written before it goes to the caller: the caller's own
+// device buffer, else the CG direction-product buffer q, dead between solves
+// and at least 18 x 4 B per voxel (>= the 8 B per voxel of a gradient).
+double* grad_target(femh_handle* H, double* user, int user_on_device) {
+  return user_on_device ? user : (double*)H->cg_q;
+}
+
+// Extents of every multigrid level of one cell (x, y, z per level, finest
+// first): halve while every extent is even and >= 4 and the level has more
+// than coarse_max_nodes nodes.  Jacobi-PCG: the cell alone.
+std::vector<int> level_dims(const femh_config& c, int nx, int ny, int nz) {
+  std::vector<int> d = {nx, ny, nz};
+  if (c.solver != FEMH_GMG_PCG) return d;
+  while ((long long)nx * ny * nz > c.coarse_max_nodes && nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0 && nx >= 4 &&
+         ny >= 4 && nz >= 4) {
+    nx /= 2; ny /= 2; nz /= 2;
+    d.insert(d.end(), {nx, ny, nz});
+  }
+  if ((long long)nx * ny * nz * 3 > 3 * 1536)
+    throw FemhError{FEMH_E_ARG, "multigrid needs cells that halve down to <= 1536 coarse nodes; use Jacobi-PCG"};
+  return d;
+}
+
+// Device bytes that build_setup allocates for one cell under config c: its
+// multigrid levels, dense coarse matrices and fine-level solver vectors (unit
+// tables and per-unit partial sums add well under 1%).  Mirrors build_setup.
+double cell_setup_bytes(const femh_config& c, int nx, int ny, int nz) {
+  const bool mixed = c.precision == FEMH_MIXED;
+  const bool gmg = c.solver == FEMH_GMG_PCG;
+  const bool mg32 = c.precision != FEMH_FP64;
+  const double vsz = mixed ? 4 : 8, msz = mg32 ? 4 : 8, csz = mg32 ? 4 : 8;
+  const double psz = c.precision == FEMH_FP64 ? 8 : (c.store_bf16 ? 2 : 4);
+  const std::vector<int> d = level_dims(c, nx, ny, nz);
+  const int nl = (int)d.size() / 3;
+  double b = 0.0;
+  for (int l = 0; l < nl; ++l) {
+    const double n = (double)d[3 * l] * d[3 * l + 1] * d[3 * l + 2];
+    b += n * (csz + 4.0);                                   // kc, invd
+    if (l > 0 || gmg) b += n * 36.0 * msz;                 // xa, xb
+    if (l > 0) b += n * 18.0 * msz;                        // bv
+    if (gmg && l == nl - 1) b += 2.0 * (3.0 * n) * (3.0 * n) * 8.0;   // coarse A, Awork
+  }
+  const double nv = (double)nx * ny * nz;
+  b += nv * (3 * 8.0 + 18 * 8.0 * 2);                      // rho_in, rho_used, kc64, b64, x64
+  if (mixed) b += nv * 18 * (8.0 + vsz);                   // r64, cg_x
+  b += nv * 18 * (2 * vsz + psz);                          // cg_r, cg_q, cg_p
+  if (c.precision == FEMH_MIXED_PC && gmg) b += nv * 18 * 4.0;   // cg_rm
+  return b;
+}
+
 void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vector<double>& hs) {
   const femh_config& c = H->cfg;
   const bool mixed = c.precision == FEMH_MIXED;
@@ -835,6 +914,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
       H->bf16_key == c.store_bf16)
     return;
   H->setup.release();
+  release_stage(H);
   H->levels.clear();
   H->solved = false;
   H->have_x = false;
@@ -863,19 +943,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
 
   // ---- levels
   std::vector<std::vector<int>> dims(nc);   // per cell: level dims
-  for (int i = 0; i < nc; ++i) {
-    int nx = shapes[3 * i], ny = shapes[3 * i + 1], nz = shapes[3 * i + 2];
-    dims[i] = {nx, ny, nz};
-    if (gmg) {
-      while ((long long)nx * ny * nz > c.coarse_max_nodes && nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0 &&
-             nx >= 4 && ny >= 4 && nz >= 4) {
-        nx /= 2; ny /= 2; nz /= 2;
-        dims[i].insert(dims[i].end(), {nx, ny, nz});
-      }
-      if ((long long)nx * ny * nz * 3 > 3 * 1536)
-        throw FemhError{FEMH_E_ARG, "multigrid needs cells that halve down to <= 1536 coarse nodes; use Jacobi-PCG"};
-    }
-  }
+  for (int i = 0; i < nc; ++i) dims[i] = level_dims(c, shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2]);
   int nlev = 1;
   for (int i = 0; i < nc; ++i) nlev = std::max(nlev, (int)dims[i].size() / 3);
   H->levels.resize(nlev);
@@ -1018,7 +1086,6 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   H->d_part_e = ar.arr<double>(L0.all.nu.size() * 22);   // 21 pair energies + sum of rho per slot
   H->d_C = ar.arr<double>(nc * 36);
   H->d_W = ar.arr<double>(nc * 21);
-  H->d_out = ar.arr<double>(21 * nv);
   H->d_nrm = ar.arr<double>(nc * kNumRhs);
   H->shape_key = shapes;
   H->h_key = hs;
@@ -1262,7 +1329,7 @@ void prepare_operator(femh_handle* H) {
     Prof prof_(H, "k_coef", 0.0);
     k_coef<TC><<<(unsigned)L0.all.nu.size(), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->rho_in, law, H->kc64,
                                                         std::is_same<TC, double>::value ? nullptr : (TC*)L0.kc,
-                                                        H->rho_used);
+                                                        H->rho_used, H->d_err + 1);
     LAUNCH_CHECK(H);
   }
   if (std::is_same<TC, double>::value)
@@ -1682,6 +1749,20 @@ void norms_of(femh_handle* H, const double* v, std::vector<double>& n2) {
   CK(cudaStreamSynchronize(s));
 }
 
+// k_coef flags a NaN, infinite or negative density (d_err[1]): an argument
+// error, reported before any solve uses the clamped stand-in value.
+void check_density(femh_handle* H) {
+  int bad = 0;
+  CK(cudaMemcpyAsync(&bad, H->d_err + 1, sizeof(int), cudaMemcpyDeviceToHost, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  if (bad) {
+    CK(cudaMemsetAsync(H->d_err + 1, 0, sizeof(int), H->stream));
+    H->have_x = false;
+    H->solved = false;
+    throw FemhError{FEMH_E_ARG, "density is NaN, infinite or negative in at least one voxel"};
+  }
+}
+
 // Solve all six load cases of all cells; fills per-cell infos (status etc.).
 void solve_all(femh_handle* H, std::vector<femh_solve_info>& infos) {
   const femh_config& c = H->cfg;
@@ -1695,7 +1776,8 @@ void solve_all(femh_handle* H, std::vector<femh_solve_info>& infos) {
   else prepare_operator<float>(H);
   const float* kc32 = (const float*)L0.kc;
   std::vector<double> bn2;
-  norms_of(H, H->b64, bn2);
+  norms_of(H, H->b64, bn2);   // synchronises: the density check below costs no extra wait
+  check_density(H);
   std::vector<double> rn2;
   int outer_done = 0;
   std::vector<int> final_status(nc * kNumRhs, CG_CONVERGED);
@@ -1978,8 +2060,22 @@ femh_status femh_create(femh_handle** out, const femh_config* cfg) {
     H->d_K0 = H->perm.arr<double>(576);
     CK(cudaMemcpy(H->d_ec, &H->ec, sizeof(ElemConst), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(H->d_K0, H->K0, sizeof(double) * 576, cudaMemcpyHostToDevice));
-    H->d_err = H->perm.arr<int>(1);
-    CK(cudaMemset(H->d_err, 0, sizeof(int)));
+    H->d_err = H->perm.arr<int>(2);
+    CK(cudaMemset(H->d_err, 0, 2 * sizeof(int)));
+    // FEMH_STAGE_WAIT_LIMIT (tests only): fewer try_wait rounds per stage wait
+    // of the bulk-copy staged kernels, so that a wait runs out although its
+    // copies complete -- the kernel then drains them with the full limit, flags
+    // the handle and returns, and the call reports FEMH_E_CUDA
+    if (const char* w = std::getenv("FEMH_STAGE_WAIT_LIMIT")) {
+      const long v = std::strtol(w, nullptr, 10);
+      if (v >= 0 && v < kWaitLimit) H->wait_limit = (int)v;
+    }
+    // FEMH_ARENA_LIMIT_BYTES (tests only): the handle's set-up allocations fail
+    // with FEMH_E_OOM beyond this many bytes, as on a device without room
+    if (const char* w = std::getenv("FEMH_ARENA_LIMIT_BYTES")) {
+      const long long v = std::strtoll(w, nullptr, 10);
+      if (v > 0) H->setup.limit = (size_t)v;
+    }
   });
   if (st != FEMH_OK) {
     femh_destroy(H);
@@ -1994,6 +2090,7 @@ femh_status femh_destroy(femh_handle* H) {
   cudaSetDevice(H->device);
   if (H->stream) cudaStreamSynchronize(H->stream);
   H->setup.release();
+  release_stage(H);
   H->perm.release();
   if (H->ev0) cudaEventDestroy(H->ev0);
   if (H->ev1) cudaEventDestroy(H->ev1);
@@ -2061,7 +2158,7 @@ femh_status femh_homogenize_batch(femh_handle* H, int ncell, const femh_cell* ce
       a.rho = H->rho_used;
       a.ec = H->d_ec;
       a.W = H->d_W;
-      a.out = H->d_out;
+      a.out = grad_target(H, dLdrho, 0);
       a.ntot = L0.ntot;
       a.k = H->hk;
       a.law = make_law(H->cfg);
@@ -2070,7 +2167,7 @@ femh_status femh_homogenize_batch(femh_handle* H, int ncell, const femh_cell* ce
         k_energy<EN_GRAD><<<(unsigned)L0.all.nu.size(), 128, 0, H->stream>>>(a);
         LAUNCH_CHECK(H);
       }
-      to_host_or_dev(H, dLdrho, H->d_out, H->nvox, 0);
+      to_host_or_dev(H, dLdrho, a.out, H->nvox, 0);
     }
   });
   return st != FEMH_OK ? st : code;
@@ -2096,7 +2193,7 @@ femh_status femh_homogenize_grad(femh_handle* H, const double dLdC[36], double* 
     a.rho = H->rho_used;
     a.ec = H->d_ec;
     a.W = H->d_W;
-    a.out = H->d_out;
+    a.out = grad_target(H, dLdrho, out_on_device);
     a.ntot = L0.ntot;
     a.k = H->hk;
     a.law = make_law(H->cfg);
@@ -2105,7 +2202,7 @@ femh_status femh_homogenize_grad(femh_handle* H, const double dLdC[36], double* 
       k_energy<EN_GRAD><<<(unsigned)L0.all.nu.size(), 128, 0, H->stream>>>(a);
       LAUNCH_CHECK(H);
     }
-    to_host_or_dev(H, dLdrho, H->d_out, H->nvox, out_on_device);
+    if (!out_on_device) to_host_or_dev(H, dLdrho, a.out, H->nvox, 0);
   });
 }
 
@@ -2146,7 +2243,7 @@ femh_status femh_dCdrho(femh_handle* H, double* out, int out_on_device) {
     a.kc64 = H->kc64;
     a.rho = H->rho_used;
     a.ec = H->d_ec;
-    a.out = H->d_out;
+    a.out = out_on_device ? out : stage(H, 21 * (size_t)H->nvox);
     a.ntot = L0.ntot;
     a.k = H->hk;
     a.law = make_law(H->cfg);
@@ -2155,7 +2252,7 @@ femh_status femh_dCdrho(femh_handle* H, double* out, int out_on_device) {
       k_energy<EN_DCDRHO><<<(unsigned)L0.all.nu.size(), 128, 0, H->stream>>>(a);
       LAUNCH_CHECK(H);
     }
-    to_host_or_dev(H, out, H->d_out, 21 * H->nvox, out_on_device);
+    if (!out_on_device) to_host_or_dev(H, out, a.out, 21 * H->nvox, 0);
   });
 }
 
@@ -2167,8 +2264,7 @@ femh_status femh_full_field(femh_handle* H, int I, double* u_out, int out_on_dev
     CK(cudaSetDevice(H->device));
     const CellDesc& cd = H->levels[0].cells[0];
     const long long n = 3LL * (cd.nx + 1) * (cd.ny + 1) * (cd.nz + 1);
-    double* tmp = H->d_out;   // 21*nvox >= 3 (n+1)^3 for n >= 2
-    if (n > 21 * H->nvox) throw FemhError{FEMH_E_ARG, "cell too small for the full-field buffer"};
+    double* tmp = stage(H, (size_t)n);
     {
       Prof prof_(H, "k_full_field", 0.0);
       k_full_field<<<cdiv(n / 3, 256), 256, 0, H->stream>>>(H->levels[0].d_cells, 0, H->x64, I, tmp,
@@ -2186,7 +2282,7 @@ femh_status femh_fluctuation(femh_handle* H, double* chi_out, int out_on_device)
     if (!chi_out) throw FemhError{FEMH_E_ARG, "chi_out must not be NULL"};
     CK(cudaSetDevice(H->device));
     const long long nn = H->nvox;
-    double* tmp = H->d_out;
+    double* tmp = stage(H, 18 * (size_t)nn);
     {
       Prof prof_(H, "k_layout", 0.0);
       k_layout<true><<<cdiv(18 * nn, 256), 256, 0, H->stream>>>(H->x64, tmp, 0, nn, H->levels[0].ntot);
@@ -2216,13 +2312,15 @@ femh_status femh_apply_operator(femh_handle* H, int nx, int ny, int nz, double h
       Prof prof_(H, "k_coef", 0.0);
       if (f32)
         k_coef<float><<<(unsigned)L0.all.nu.size(), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->rho_in, law, H->kc64,
-                                                               (float*)L0.kc, H->rho_used);
+                                                               (float*)L0.kc, H->rho_used, H->d_err + 1);
       else
         k_coef<double><<<(unsigned)L0.all.nu.size(), 256, 0, s>>>(L0.d_cells, L0.all.d_nu, H->rho_in, law,
-                                                                H->kc64, (double*)nullptr, H->rho_used);
+                                                                H->kc64, (double*)nullptr, H->rho_used,
+                                                                H->d_err + 1);
       LAUNCH_CHECK(H);
     }
-    double* tmp = H->d_out;
+    check_density(H);
+    double* tmp = stage(H, 18 * (size_t)nn);
     H->have_x = false;   // x64 serves as the input buffer below
     CK(cudaMemcpyAsync(tmp, u, sizeof(double) * 18 * nn, k_in, s));
     {
@@ -2253,6 +2351,23 @@ femh_status femh_apply_operator(femh_handle* H, int nx, int ny, int nz, double h
     }
     to_host_or_dev(H, y, tmp, 18 * nn, on_device);
     H->solved = false;
+  });
+}
+
+femh_status femh_batch_memory(femh_handle* H, int ncell, const femh_cell* cells, double* need_bytes,
+                              double* avail_bytes) {
+  if (!H) return FEMH_E_ARG;
+  return guard(H, [&] {
+    if (ncell < 0 || (ncell > 0 && !cells)) throw FemhError{FEMH_E_ARG, "ncell >= 0 and cells are required"};
+    double need = 0.0;
+    for (int i = 0; i < ncell; ++i) need += cell_setup_bytes(H->cfg, cells[i].nx, cells[i].ny, cells[i].nz);
+    if (need_bytes) *need_bytes = need;
+    if (avail_bytes) {
+      CK(cudaSetDevice(H->device));
+      size_t fr = 0, tot = 0;
+      CK(cudaMemGetInfo(&fr, &tot));
+      *avail_bytes = (double)fr + (double)H->setup.held + (double)H->stage_n * sizeof(double);
+    }
   });
 }
 

@@ -57,14 +57,20 @@ __device__ __forceinline__ int wrap(int a, int n) { return a < 0 ? a + n : (a >=
 
 // ---------------------------------------------------------------- setup ---
 // Fine-level stiffness scale kc[e] = E(clamp(rho_e)) * h and the rho actually used.
+// A density that is NaN, infinite or negative is not clamped into range but
+// reported: *bad = 1 (the host turns it into FEMH_E_ARG before solving).
 template <typename TC2>
 __global__ void k_coef(const CellDesc* cells, const NodeUnit* units, const double* rho, MatLaw law,
-                       double* kc64, TC2* kc2, double* rho_used) {
+                       double* kc64, TC2* kc2, double* rho_used, int* bad) {
   const NodeUnit u = units[blockIdx.x];
   const CellDesc cd = cells[u.cell];
   #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
     double r = rho[cd.off + n];
+    if (!(r >= 0.0) || isinf(r)) {
+      *bad = 1;
+      r = 0.0;
+    }
     r = fmin(fmax(r, law.rho_min), law.rho_max);
     const double kc = law_coef(law, r) * cd.h;
     if (rho_used) rho_used[cd.off + n] = r;

@@ -50,6 +50,7 @@ struct StencilArgs {
   double omega;
   float2 kp[8];          // FP32 pairs (x = y) of A, Bd-Bo, Bo, D1-O1, O1, D2-O2, O2, G
   int* err;              // set non-zero by a kernel whose bounded wait ran out
+  int wait_limit;        // try_wait rounds of a stage wait (kWaitLimit; smaller only in tests)
 };
 
 template <typename T>
@@ -1233,9 +1234,10 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
   return ok != 0;
 }
 // Bounded wait for a phase of an mbarrier: false if it did not complete
-// within the iteration limit (each try_wait also suspends for a while).
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-  for (int it = 0; it < (1 << 20); ++it)
+// within `limit` try_wait rounds (each also suspends for a while).
+constexpr int kWaitLimit = 1 << 20;
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int limit = kWaitLimit) {
+  for (int it = 0; it < limit; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -1361,13 +1363,14 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
   __syncthreads();
   if (tid < 32)
     for (int g = 0; g < kBulkSlots && g < G; ++g) issue(g);
-  int waited = 0;   // stages this thread has waited for (for the exit drain)
+  int waited = 0;   // stages 0 .. waited-1 completed for this thread (the exit drain starts there)
   auto wait_stage = [&](int g) {
-    if (!mbar_wait(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1))) {
+    if (!mbar_wait(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1), a.wait_limit)) {
       if (a.err) atomicExch(a.err, 1);
       abort_flag = 1;
+    } else if (waited == g) {
+      waited = g + 1;   // a stage that timed out stays owed to the drain
     }
-    waited = g + 1;
   };
 
   f2 prv[3][4], car[3][4];
@@ -1668,13 +1671,14 @@ stencil1b_kernel(StencilArgs<TIn, double, double, double> a) {
   __syncthreads();
   if (tid < 32)
     for (int g = 0; g < kBulkSlots && g < G; ++g) issue(g);
-  int waited = 0;
+  int waited = 0;   // stages 0 .. waited-1 completed for this thread (the exit drain starts there)
   auto wait_stage = [&](int g) {
-    if (!mbar_wait(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1))) {
+    if (!mbar_wait(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1), a.wait_limit)) {
       if (a.err) atomicExch(a.err, 1);
       abort_flag = 1;
+    } else if (waited == g) {
+      waited = g + 1;   // a stage that timed out stays owed to the drain
     }
-    waited = g + 1;
   };
 
   double prv[3][4], car[3][4];

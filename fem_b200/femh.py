@@ -32,7 +32,7 @@ EXPORTS = (
     "femh_config_default", "femh_create", "femh_destroy", "femh_homogenize", "femh_homogenize_grad",
     "femh_dCdrho", "femh_force_tensors", "femh_full_field", "femh_fluctuation", "femh_apply_operator", "femh_homogenize_batch",
     "femh_last_error", "femh_set_stream", "femh_kernel_launches", "femh_profile", "femh_profile_read",
-    "femh_energy_noalloc",
+    "femh_energy_noalloc", "femh_batch_memory",
 )
 
 
@@ -106,6 +106,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.femh_profile.argtypes = [vp, ip]
     L.femh_profile_read.argtypes = [vp, ctypes.POINTER(_KStat), ip, ctypes.POINTER(ctypes.c_int)]
     L.femh_energy_noalloc.argtypes = [ctypes.POINTER(_Config), ip, ip, ip, ctypes.c_double, vp, vp, vp, vp]
+    L.femh_batch_memory.argtypes = [vp, ip, ctypes.POINTER(_Cell), dp, dp]
     _lib = L
     return L
 
@@ -289,26 +290,45 @@ class Engine:
         self._ncells = 0
         return y
 
+    def batch_memory(self, shapes: Sequence[tuple]) -> tuple[list[float], float]:
+        """Device bytes a batch call needs for each cell shape, and the bytes
+        available to it (femh_batch_memory)."""
+        need, avail = [], ctypes.c_double()
+        for i, (nx, ny, nz) in enumerate(shapes):
+            c = _Cell()
+            c.nx, c.ny, c.nz, c.h = int(nx), int(ny), int(nz), 1.0
+            b = ctypes.c_double()
+            self._check(self.lib.femh_batch_memory(self.h, 1, ctypes.byref(c), ctypes.byref(b),
+                                                   ctypes.byref(avail) if i == 0 else None))
+            need.append(b.value)
+        return need, avail.value
+
     def batch(self, rhos: Sequence[np.ndarray], h: float | None = None, dLdC=None, allow_unconverged=False,
               max_nodes: int | None = None):
         """Many cells in one set of launches.  Returns (C [n,6,6], infos, dLdrho list or None).
 
-        max_nodes: split the cells into consecutive calls of at most that many
-        voxels each (at least one cell per call); the engine keeps about 1.1 KB
-        per voxel in the mixed mode, so a call that does not fit the GPU's
-        memory fails with FEMH_E_OOM.  After a split call force_tensors() is
-        not available (the engine holds only the last part's fields)."""
-        if max_nodes is not None and sum(int(np.prod(r.shape)) for r in rhos) > max_nodes:
+        The cells go to the engine in consecutive calls (at least one cell per
+        call) of at most ``max_nodes`` voxels each, or by default of what fits
+        the device (femh_batch_memory's estimate against 92% of the memory
+        available; the whole set when it fits).  After a split call
+        force_tensors() is not available (the engine holds only the last
+        part's fields)."""
+        sizes = [int(np.prod(r.shape)) for r in rhos]
+        if max_nodes is None:
+            need, avail = self.batch_memory([r.shape for r in rhos])
+            cost, budget = need, 0.92 * avail
+        else:
+            cost, budget = sizes, max_nodes
+        if sum(cost) > budget:
             dl = None if dLdC is None else np.ascontiguousarray(dLdC, dtype=np.float64).reshape(len(rhos), 6, 6)
             Cs, infos, grads = [], [], ([] if dLdC is not None else None)
             i = 0
             while i < len(rhos):
-                j, nodes = i, 0
-                while j < len(rhos) and (j == i or nodes + int(np.prod(rhos[j].shape)) <= max_nodes):
-                    nodes += int(np.prod(rhos[j].shape))
+                j, used = i, 0.0
+                while j < len(rhos) and (j == i or used + cost[j] <= budget):
+                    used += cost[j]
                     j += 1
-                C, inf, g = self.batch(rhos[i:j], h=h, dLdC=None if dl is None else dl[i:j],
-                                       allow_unconverged=allow_unconverged)
+                C, inf, g = self._batch1(rhos[i:j], h, None if dl is None else dl[i:j], allow_unconverged)
                 Cs.append(C)
                 infos += inf
                 if grads is not None:
@@ -316,6 +336,9 @@ class Engine:
                 i = j
             self._ncells = 0
             return np.concatenate(Cs), infos, grads
+        return self._batch1(rhos, h, dLdC, allow_unconverged)
+
+    def _batch1(self, rhos, h, dLdC, allow_unconverged):
         n = len(rhos)
         rhos = [np.ascontiguousarray(r, dtype=np.float64) for r in rhos]
         cells = (_Cell * n)()

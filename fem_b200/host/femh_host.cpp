@@ -19,10 +19,17 @@ void check(femh_handle* h, int st, bool allow_unconverged = false) {
   throw Error(st, "femh error " + std::to_string(st) + ": " + buf);
 }
 
-// Structures of n[0] x n[1] x n[2] voxels per batched engine call, at least one.
-size_t batch_cells_per_call(const int n[3], long long max_nodes) {
+// Structures of n[0] x n[1] x n[2] voxels per batched engine call, at least
+// one: a voxel budget when max_nodes > 0, else what fits the device -- the
+// engine's estimate of one cell's memory against 92% of the memory available
+// to the handle (femh_batch_memory).
+size_t batch_cells_per_call(femh_handle* h, const int n[3], long long max_nodes) {
   const long long cell = (long long)n[0] * n[1] * n[2];
-  return (size_t)std::max(1LL, max_nodes / std::max(1LL, cell));
+  if (max_nodes > 0) return (size_t)std::max(1LL, max_nodes / std::max(1LL, cell));
+  femh_cell c{n[0], n[1], n[2], 1.0, nullptr};
+  double need = 0.0, avail = 0.0;
+  check(h, femh_batch_memory(h, 1, &c, &need, &avail));
+  return (size_t)std::max(1.0, std::floor(0.92 * avail / std::max(need, 1.0)));
 }
 }  // namespace
 
@@ -218,9 +225,9 @@ void NumericalCoarseningUsingMultigrid::init(int N[3], int iNbBlockRep, int iNbS
 void NumericalCoarseningUsingMultigrid::append(const double C[36], const std::vector<int>& mats,
                                                const std::vector<double>& dens, StructureType t,
                                                std::vector<double>& tv, std::vector<double>& pv) {
-  for (int i = 0; i < 6; ++i)
-    for (int j = 0; j <= i; ++j) tv.push_back(C[i * 6 + j]);
   if (t != Cubic) throw Error(FEMH_E_ARG, "only Cubic structures derive (rho, E, nu, G), as in the reference");
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j <= i; ++j) tv.push_back(referenceLowerTriangle && j < i ? 0.0 : C[i * 6 + j]);
   double r = 0.0;
   for (int m : mats) r += dens.at(m);
   r /= (double)mats.size();
@@ -257,7 +264,8 @@ void NumericalCoarseningUsingMultigrid::computeBatch(const std::vector<std::vect
   if (nc == 0) return;
   const int n[3] = {N[0] * m_nbBlockRep * m_nbSubdiv, N[1] * m_nbBlockRep * m_nbSubdiv,
                     N[2] * m_nbBlockRep * m_nbSubdiv};
-  const size_t per = batch_cells_per_call(n, maxNodesPerCall);
+  const size_t per = batch_cells_per_call(h_, n, maxNodesPerCall);
+  std::vector<double> tv_new, pv_new;   // appended to the caller's vectors once every call succeeded
   for (size_t c0 = 0; c0 < nc; c0 += per) {
     const size_t m = std::min(per, nc - c0);
     std::vector<std::vector<double>> rho(m);
@@ -273,9 +281,11 @@ void NumericalCoarseningUsingMultigrid::computeBatch(const std::vector<std::vect
     std::vector<double> C(36 * m);
     std::vector<femh_solve_info> infos(m);
     check(h_, femh_homogenize_batch(h_, (int)m, cells.data(), C.data(), nullptr, nullptr, infos.data()), true);
-    for (size_t c = 0; c < m; ++c) append(&C[36 * c], iMaterials[c0 + c], iDens, t, tv, pv);
+    for (size_t c = 0; c < m; ++c) append(&C[36 * c], iMaterials[c0 + c], iDens, t, tv_new, pv_new);
     lastInfo = infos.back();
   }
+  tv.insert(tv.end(), tv_new.begin(), tv_new.end());
+  pv.insert(pv.end(), pv_new.begin(), pv_new.end());
 }
 
 // ---------------------------------------------------------- NumericalCoarsening
@@ -392,7 +402,8 @@ void NumericalCoarsening::computeBatch(const std::vector<std::vector<int>>& iMat
   const int n[3] = {N[0] * m_nbBlockRep * m_nbSubdiv, N[1] * m_nbBlockRep * m_nbSubdiv,
                     N[2] * m_nbBlockRep * m_nbSubdiv};
   const double dx = 1.0 / std::max(n[0], std::max(n[1], n[2]));
-  const size_t per = batch_cells_per_call(n, maxNodesPerCall);
+  const size_t per = batch_cells_per_call(h_, n, maxNodesPerCall);
+  std::vector<double> tv_new, pv_new;   // appended to the caller's vectors once every call succeeded
   for (size_t c0 = 0; c0 < nc; c0 += per) {
     const size_t m = std::min(per, nc - c0);
     std::vector<std::vector<double>> rho(m);
@@ -408,9 +419,12 @@ void NumericalCoarsening::computeBatch(const std::vector<std::vector<int>>& iMat
     std::vector<femh_solve_info> infos(m);
     check(h_, femh_homogenize_batch(h_, (int)m, cells.data(), CH.data(), nullptr, nullptr, infos.data()), true);
     check(h_, femh_force_tensors(h_, Cf.data()));
-    for (size_t c = 0; c < m; ++c) append(&CH[36 * c], &Cf[36 * c], n, iMaterials[c0 + c], iDens, t, tv, pv);
+    for (size_t c = 0; c < m; ++c)
+      append(&CH[36 * c], &Cf[36 * c], n, iMaterials[c0 + c], iDens, t, tv_new, pv_new);
     lastInfo = infos.back();
   }
+  tv.insert(tv.end(), tv_new.begin(), tv_new.end());
+  pv.insert(pv.end(), pv_new.begin(), pv_new.end());
 }
 
 // ------------------------------------------------------------ binary files

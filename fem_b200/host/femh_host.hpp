@@ -130,15 +130,22 @@ class NumericalCoarseningUsingMultigrid {
                                                        const std::vector<double>& iBaseMaterialDensities,
                                                        StructureType iType, std::vector<double>& ioTensorValues,
                                                        std::vector<double>& ioParameters);
-  // Many structures in batched engine calls (the sample generator's batch),
-  // split so that one call holds at most maxNodesPerCall voxels (the engine
-  // keeps about 1.1 KB per voxel in the mixed mode: 64M voxels ~ 70 GB).
+  // Many structures in batched engine calls (the sample generator's batch).
+  // maxNodesPerCall > 0 caps the voxels of one call; 0 (default) splits by
+  // what fits the device (femh_batch_memory).  The outputs are appended only
+  // once every call has succeeded: on an error they are left as they were.
   void computeBatch(const std::vector<std::vector<int>>& iMaterials, int N[3],
                     const std::vector<double>& iBaseMaterialDensities, StructureType iType,
                     std::vector<double>& ioTensorValues, std::vector<double>& ioParameters);
 
   femh_solve_info lastInfo{};
-  long long maxNodesPerCall = 64LL << 20;
+  long long maxNodesPerCall = 0;
+  // The reference fills only the upper triangle of its C but appends the
+  // entries C(i, j), j <= i (NumericalCoarseningUsingMultiGrid.cpp:296-324), so
+  // its 15 off-diagonal tensor values are 0.  false (default): append the
+  // symmetric tensor's values; true: append those zeros, as the reference's
+  // tensor files hold them (the parameters use C(0,1) either way, as there).
+  bool referenceLowerTriangle = false;
 
  private:
   femh_handle* h_ = nullptr;
@@ -182,13 +189,15 @@ class NumericalCoarsening {
                                                        const std::vector<double>& iBaseMaterialDensities,
                                                        StructureType iType, std::vector<double>& ioTensorValues,
                                                        std::vector<double>& ioParameters);
-  // Many structures in batched engine calls of at most maxNodesPerCall voxels.
+  // Many structures in batched engine calls; maxNodesPerCall as in
+  // NumericalCoarseningUsingMultigrid::computeBatch (0: what fits the device);
+  // outputs appended only once every call has succeeded.
   void computeBatch(const std::vector<std::vector<int>>& iMaterials, int N[3],
                     const std::vector<double>& iBaseMaterialDensities, StructureType iType,
                     std::vector<double>& ioTensorValues, std::vector<double>& ioParameters);
 
   femh_solve_info lastInfo{};
-  long long maxNodesPerCall = 64LL << 20;
+  long long maxNodesPerCall = 0;
 
  private:
   femh_handle* h_ = nullptr;

@@ -50,7 +50,7 @@ enum {
 };
 
 /* material law of the per-voxel Young's modulus E(rho); K0 uses nu */
-enum { FEMH_INTERP_SIMP = 0,    /* E_min + rho^p (E_s - E_min)   (BASELINE law) */
+enum { FEMH_INTERP_SIMP = 0,    /* E_min + rho^p (E_s - E_min)   MaterialOpt/src/FEM3DFun.cpp:244-257 */
        FEMH_INTERP_RAMP3 = 1,   /* E_s rho/(3-2rho)  fast_fem/FEM3DFun.cpp:20-27 */
        FEMH_INTERP_BINARY = 2   /* rho>=0.5 ? bin_hi : bin_lo
                                    NumericalCoarseningUsingMultiGrid.cpp:235-241 */ };
@@ -64,7 +64,9 @@ typedef struct {
   int interp;             /* FEMH_INTERP_* */
   double E_s, E_min, penal, nu;
   double bin_hi, bin_lo;
-  double rho_min, rho_max; /* clamp applied before the law (fast_fem clamps 1e-3..1) */
+  double rho_min, rho_max; /* clamp applied before the law (fast_fem clamps 1e-3..1); a
+                              density that is NaN, infinite or negative is not clamped but
+                              rejected: the solve returns FEMH_E_ARG */
   int precision;          /* FEMH_FP64 | FEMH_MIXED | FEMH_MIXED_PC */
   int solver;             /* FEMH_JACOBI_PCG | FEMH_GMG_PCG */
   int pre_smooth, post_smooth; /* damped-Jacobi sweeps per level (GMG); equal counts keep the
@@ -190,6 +192,17 @@ femh_status femh_apply_operator(femh_handle* h, int nx, int ny, int nz, double h
  * All pointers host-side. */
 femh_status femh_homogenize_batch(femh_handle* h, int ncell, const femh_cell* cells, double* C_out,
                                   const double* dLdC, double* dLdrho, femh_solve_info* infos);
+
+/* Device memory a femh_homogenize_batch call on these cells needs under the
+ * handle's configuration (need_bytes: multigrid levels, coarse matrices and
+ * solver vectors; about 0.9 KB per voxel in FEMH_MIXED_PC, 1.1 KB in FEMH_FP64),
+ * and what is available to it (avail_bytes: free device memory plus what the
+ * handle itself holds, which the call would release first).  Either output may
+ * be NULL.  For splitting a cell set that does not fit one call (the sample
+ * generator's batches); no counterpart in the reference, whose per-cell
+ * PARDISO solves never hold more than one cell. */
+femh_status femh_batch_memory(femh_handle* h, int ncell, const femh_cell* cells, double* need_bytes,
+                              double* avail_bytes);
 
 /* Copy the last error message (NUL-terminated) into buf. */
 femh_status femh_last_error(const femh_handle* h, char* buf, size_t n);

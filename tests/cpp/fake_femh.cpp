@@ -1,4 +1,4 @@
-// A stand-in for libfemh's C ABI (test double, no GPU): the eight entry points
+// A stand-in for libfemh's C ABI (test double, no GPU): the nine entry points
 // the C++ host layer calls, returning deterministic tensors so that the host
 // layer's own logic -- material mapping, repMaterialAssignment, parameter
 // formulas, batch bookkeeping, error paths -- can be checked on the CPU.
@@ -22,7 +22,9 @@ struct femh_handle {
   int nvox = 0;
 };
 
-int g_batch_calls = 0;   // femh_homogenize_batch calls so far (read by the test driver)
+int g_batch_calls = 0;        // femh_homogenize_batch calls so far (read by the test driver)
+int g_fail_batch_call = -1;   // that call (by count) returns FEMH_E_OOM, as a batch too large would
+double g_fake_avail = 1e12;   // device bytes femh_batch_memory reports available
 
 namespace {
 void fake_C(const femh_config& c, int nx, int ny, int nz, const double* rho, double C[36]) {
@@ -87,7 +89,10 @@ femh_status femh_homogenize(femh_handle* h, int nx, int ny, int nz, double, cons
 femh_status femh_homogenize_batch(femh_handle* h, int ncell, const femh_cell* cells, double* C_out,
                                   const double*, double*, femh_solve_info* infos) {
   if (!h || ncell < 1 || !cells || !C_out) return FEMH_E_ARG;
-  ++g_batch_calls;
+  if (++g_batch_calls == g_fail_batch_call) {
+    h->err = "out of device memory (test double)";
+    return FEMH_E_OOM;
+  }
   h->C.clear();
   h->cubic.clear();
   for (int i = 0; i < ncell; ++i) {
@@ -121,6 +126,16 @@ femh_status femh_homogenize_grad(femh_handle* h, const double dLdC[36], double* 
   double t = 0.0;
   for (int a = 0; a < 6; ++a) t += dLdC[7 * a];
   for (int i = 0; i < h->nvox; ++i) dLdrho[i] = t;
+  return FEMH_OK;
+}
+
+// 1000 bytes per voxel; g_fake_avail available
+femh_status femh_batch_memory(femh_handle* h, int ncell, const femh_cell* cells, double* need, double* avail) {
+  if (!h || ncell < 0 || (ncell > 0 && !cells)) return FEMH_E_ARG;
+  double b = 0.0;
+  for (int i = 0; i < ncell; ++i) b += 1000.0 * cells[i].nx * cells[i].ny * cells[i].nz;
+  if (need) *need = b;
+  if (avail) *avail = g_fake_avail;
   return FEMH_OK;
 }
 

@@ -84,6 +84,39 @@ int main(int argc, char** argv) {
   print_vec("x0", x0);
   print_vec("df_fd", fd);
   print_vec("df_adjoint", an);
+  // ------------------------------------------------------------- 1b
+  // an 8^3 cell over a 4^3 PiecewiseConstant3D field (the field chain rule sums
+  // eight voxels per parameter), parameters partly outside [1e-3, 1] (setParam
+  // clamps), upper-triangular weights: the test compares G, f and df with the
+  // reference's own FEM3DFun (oracle/_ref/libfastfem_ref.so)
+  {
+    PiecewiseConstant3D f4;
+    f4.allocate(4, 4, 4);
+    std::vector<double> x4(64);
+    for (int i = 0; i < 64; ++i) x4[i] = -0.1 + 1.2 * ((i * 37 + 11) % 64) / 63.0;
+    FEM3DFun fb;
+    fb.gridSize = {n, n, n};
+    fb.field = &f4;
+    fb.E = 1.0;
+    fb.nu = 0.3;
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j < 6; ++j) {
+        fb.wG[i * 6 + j] = j >= i ? 0.5 + ((i * 5 + j * 3) % 7) / 7.0 : 0.0;
+        fb.G0[i * 6 + j] = (i == j) ? (i < 3 ? 0.1 : 0.03) : (j > i ? 0.01 : 0.0);
+      }
+    fb.m0 = 0.4;
+    fb.mw = 0.1;
+    fb.init(x4);
+    fb.setParam(x4);
+    const double fv = fb.f();
+    std::vector<double> gb = fb.df();
+    std::printf("\"ff_f\": %.17g,\n", fv);
+    print_vec("ff_x0", x4);
+    print_vec("ff_G", std::vector<double>(fb.G.begin(), fb.G.end()));
+    print_vec("ff_G0", std::vector<double>(fb.G0.begin(), fb.G0.end()));
+    print_vec("ff_wG", std::vector<double>(fb.wG.begin(), fb.wG.end()));
+    print_vec("ff_df", gb);
+  }
   // ---------------------------------------------------------------- 2
   NumericalCoarseningUsingMultigrid nc;
   int N[3] = {4, 4, 4};

@@ -13,6 +13,8 @@
 using namespace femh_host;
 
 extern int g_batch_calls;   // tests/cpp/fake_femh.cpp
+extern int g_fail_batch_call;
+extern double g_fake_avail;
 
 static void print_vec(const char* key, const std::vector<double>& v) {
   std::printf("\"%s\": [", key);
@@ -56,7 +58,25 @@ int main() {
     fc.computeBatch(structs, N, dens, NumericalCoarsening::Cubic, ts, ps);
     std::printf("\"force_split_calls\": %d,\n", g_batch_calls - before);
     std::printf("\"force_split_equal\": %s,\n", (ts == tvb && ps == pvb) ? "true" : "false");
-    fc.maxNodesPerCall = 64LL << 20;
+    // default split: what fits the device -- 0.92 x 150 kB over 64 kB a cell = 2 cells per call
+    std::vector<double> ta, pa;
+    fc.maxNodesPerCall = 0;
+    g_fake_avail = 150e3;
+    const int before_auto = g_batch_calls;
+    fc.computeBatch(structs, N, dens, NumericalCoarsening::Cubic, ta, pa);
+    std::printf("\"force_auto_calls\": %d,\n", g_batch_calls - before_auto);
+    std::printf("\"force_auto_equal\": %s,\n", (ta == tvb && pa == pvb) ? "true" : "false");
+    // a failing second call (FEMH_E_OOM) leaves the caller's vectors as they were
+    std::vector<double> tk = {7.0}, pk = {8.0, 9.0};
+    fc.maxNodesPerCall = 64;
+    g_fail_batch_call = g_batch_calls + 2;
+    const int code = error_code([&] { fc.computeBatch(structs, N, dens, NumericalCoarsening::Cubic, tk, pk); });
+    g_fail_batch_call = -1;
+    std::printf("\"force_failed_code\": %d,\n", code);
+    std::printf("\"force_failed_untouched\": %s,\n",
+                (tk == std::vector<double>{7.0} && pk == std::vector<double>{8.0, 9.0}) ? "true" : "false");
+    g_fake_avail = 1e12;
+    fc.maxNodesPerCall = 0;
   }
   std::vector<double> cell0;   // structure 0 after repMaterialAssignment
   {
@@ -103,6 +123,23 @@ int main() {
     mg.computeBatch(structs, N, dens, NumericalCoarseningUsingMultigrid::Cubic, t2, p2);
     std::printf("\"mg_split_calls\": %d,\n", g_batch_calls - before);
     std::printf("\"mg_split_equal\": %s,\n", (t1 == t2 && p1 == p2) ? "true" : "false");
+    std::vector<double> tk = {1.0}, pk = {2.0};
+    g_fail_batch_call = g_batch_calls + 2;
+    const int code = error_code([&] { mg.computeBatch(structs, N, dens, NumericalCoarseningUsingMultigrid::Cubic, tk, pk); });
+    g_fail_batch_call = -1;
+    std::printf("\"mg_failed_code\": %d,\n", code);
+    std::printf("\"mg_failed_untouched\": %s,\n",
+                (tk == std::vector<double>{1.0} && pk == std::vector<double>{2.0}) ? "true" : "false");
+    mg.maxNodesPerCall = 0;
+  }
+  {   // the reference's tensor files: the 15 off-diagonal lower-triangle values are 0
+    std::vector<double> tr, pr;
+    mg.referenceLowerTriangle = true;
+    mg.computeCoarsenedElasticityTensorAndParameters3D(structs[0], N, dens, NumericalCoarseningUsingMultigrid::Cubic,
+                                                       tr, pr);
+    mg.referenceLowerTriangle = false;
+    print_vec("mg_tensors_reference_triangle", tr);
+    print_vec("mg_params_reference_triangle", pr);
   }
   // FEM3DFun objective and chain rule through a piecewise-constant field
   const int n = 4;

@@ -82,10 +82,35 @@ def test_force_driven_class(out):
 
 def test_batches_split_by_node_budget(out):
     """computeBatch splits the structures into engine calls of at most
-    maxNodesPerCall voxels (the engine's memory is about 1.1 KB per voxel) and
+    maxNodesPerCall voxels, or by default into calls that fit the device
+    (femh_batch_memory's estimate against 92% of the available memory), and
     returns the same values as one call."""
     assert out["force_split_calls"] == 3 and out["force_split_equal"]
+    assert out["force_auto_calls"] == 2 and out["force_auto_equal"]
     assert out["mg_split_calls"] == 2 and out["mg_split_equal"]
+
+
+def test_failed_batch_leaves_outputs_unchanged(out):
+    """A part of a split batch that fails (FEMH_E_OOM from the engine) raises
+    and appends nothing: the caller can retry with a smaller budget without
+    duplicate tensors."""
+    assert out["force_failed_code"] == 3 and out["force_failed_untouched"]
+    assert out["mg_failed_code"] == 3 and out["mg_failed_untouched"]
+
+
+def test_multigrid_reference_lower_triangle_switch(out):
+    """referenceLowerTriangle = true appends what the reference's tensor files
+    hold -- C(i, j), j <= i, of a C whose lower triangle it never fills
+    (SamplesGenerator/NumericalCoarseningUsingMultiGrid.cpp:296-324): the 15
+    off-diagonal values are 0, the diagonal ones and the parameters unchanged.
+    The default appends the symmetric tensor's values."""
+    ref = np.array(out["mg_tensors_reference_triangle"])
+    full = np.array(out["mg_tensors"])
+    diag = [t for t, (i, j) in enumerate((i, j) for i in range(6) for j in range(i + 1)) if i == j]
+    off = [t for t in range(21) if t not in diag]
+    assert np.all(ref[off] == 0.0) and np.any(full[off] != 0.0)
+    assert np.array_equal(ref[diag], full[diag])
+    assert out["mg_params_reference_triangle"] == out["mg_params"]
 
 
 def test_force_driven_argument_errors(out):

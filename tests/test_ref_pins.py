@@ -55,3 +55,44 @@ def test_nc_uniform_reference_is_material():
     tv, pv = R.nc_coarsen(mats, (0.5, 1.0), 0.3, (0.0, 1.0), R.CUBIC)
     mu = 1.0 / (2 * 1.3)
     assert np.allclose(pv, [1.0, 1.0, 0.3, mu], rtol=1e-4, atol=0)
+
+
+# ---------------------------------------------------------------- fast_fem FEM3DFun
+def _ff_case(n, m, seed):
+    rng = np.random.default_rng(seed)
+    x0 = rng.uniform(-0.1, 1.1, m ** 3)   # outside [1e-3, 1] too: setParam clamps
+    G0 = np.diag([0.1, 0.1, 0.1, 0.03, 0.03, 0.03]) + 0.01 * np.triu(np.ones((6, 6)), 1)
+    wG = np.triu(rng.uniform(0.5, 1.5, (6, 6)))
+    return x0, G0, wG
+
+
+@pytest.mark.skipif(not R.available("libfastfem_ref.so"), reason="oracle/_ref/libfastfem_ref.so not built")
+@pytest.mark.parametrize("n,m", [(8, 8), (8, 4), (12, 6)])
+def test_fastfem_energy_and_gradient_loops_vs_oracle(oracle, n, m):
+    """fast_fem's own setParam energy loop, f and df (field chain rule and
+    density term included, fast_fem/FEM3DFun.cpp:128-268), fed the oracle's
+    fluctuation through the stand-in topoOptLib headers, against the oracle's
+    energy and gradient restatement (fo_energy, fo_grad) on the same clamped
+    distribution: G to 1e-12, df to 1e-10 relative.  The reference fills only
+    the upper triangle of G; with upper-triangular weights its objective is the
+    symmetric one."""
+    x0, G0, wG = _ff_case(n, m, seed=n + m)
+    nu, m0, mw = 0.3, 0.4, 0.1
+    r = R.fastfem(n, x0, nu, G0, wG, m0, mw)
+    assert r["status"] == 0
+    rep = n // m
+    rho = np.clip(np.repeat(np.repeat(np.repeat(x0.reshape(m, m, m), rep, 0), rep, 1), rep, 2), 1e-3, 1.0)
+    assert np.array_equal(r["distribution"], rho)
+    assert r["density"] == pytest.approx(rho.mean(), rel=1e-14)
+    mat = oracle.material(interp=oracle.INTERP_RAMP3, E_s=1.0, nu=nu)
+    C, chi, _, _, st = oracle.homogenize(rho, mat=mat, tol=1e-12, max_iter=100000)
+    assert st == 0
+    iu = np.triu_indices(6)
+    assert np.abs(r["G"][iu] - C[iu]).max() < 1e-11 * np.abs(C).max()
+    assert np.abs(np.tril(r["G"], -1)).max() == 0.0
+    Gref = r["G"]
+    f = 0.5 * np.sum(wG * (Gref - G0) ** 2) + 0.5 * mw * (rho.mean() - m0) ** 2
+    assert r["f"] == pytest.approx(f, rel=1e-10)
+    dfd = oracle.grad(rho, chi, wG * (Gref - G0), mat=mat) + (mw / rho.size) * (rho.mean() - m0)
+    g = dfd.reshape(m, rep, m, rep, m, rep).sum(axis=(1, 3, 5)).ravel()
+    assert np.abs(r["df"] - g).max() < 1e-10 * np.abs(g).max()
