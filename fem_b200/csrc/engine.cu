@@ -396,6 +396,11 @@ struct femh_handle {
   double* d_W = nullptr;        // [ncells][21]
   double* d_stage = nullptr;    // output staging (dCdrho, fields, apply), allocated on first use
   size_t stage_n = 0;           // doubles in d_stage
+  // field chain rule: voxels of each field parameter (CSR), cached by the map's hash
+  int* d_fmap = nullptr;        // [nparam + 1] offsets, then [nmapped] voxel indices
+  size_t fmap_n = 0;            // ints allocated
+  unsigned long long fmap_key = 0;
+  int fmap_nparam = -1;
   double* d_nrm = nullptr;      // [ncells][6]
   bool solved = false;
   bool have_x = false;   // x64 holds the last solution of these cells (warm starts)
@@ -845,6 +850,11 @@ void release_stage(femh_handle* H) {
   if (H->d_stage) cudaFree(H->d_stage);
   H->d_stage = nullptr;
   H->stage_n = 0;
+  if (H->d_fmap) cudaFree(H->d_fmap);
+  H->d_fmap = nullptr;
+  H->fmap_n = 0;
+  H->fmap_key = 0;
+  H->fmap_nparam = -1;
 }
 
 double* stage(femh_handle* H, size_t n) {
@@ -2203,6 +2213,83 @@ femh_status femh_homogenize_grad(femh_handle* H, const double dLdC[36], double* 
       LAUNCH_CHECK(H);
     }
     if (!out_on_device) to_host_or_dev(H, dLdrho, a.out, H->nvox, 0);
+  });
+}
+
+femh_status femh_field_gradient(femh_handle* H, const double dLdC[36], double dLdrho_add, int nparam,
+                                const int* voxel_param, double* grad_out) {
+  if (!H) return FEMH_E_ARG;
+  return guard(H, [&] {
+    if (!H->solved || H->ncells != 1) throw FemhError{FEMH_E_STATE, "call femh_homogenize first"};
+    if (!dLdC || !voxel_param || !grad_out || nparam < 1)
+      throw FemhError{FEMH_E_ARG, "dLdC, voxel_param, grad_out and nparam >= 1 are required"};
+    CK(cudaSetDevice(H->device));
+    const long long nv = H->nvox;
+    // voxels of each parameter, in voxel order (FNV-1a hash of the map decides reuse)
+    unsigned long long key = 1469598103934665603ULL ^ (unsigned long long)nparam;
+    for (long long e = 0; e < nv; ++e) {
+      const int p = voxel_param[e];
+      if (p < -1 || p >= nparam) throw FemhError{FEMH_E_ARG, "voxel_param entries must lie in [-1, nparam)"};
+      key = (key ^ (unsigned long long)(unsigned)p) * 1099511628211ULL;
+    }
+    if (key != H->fmap_key || nparam != H->fmap_nparam) {
+      std::vector<int> ptr(nparam + 1, 0);
+      for (long long e = 0; e < nv; ++e)
+        if (voxel_param[e] >= 0) ptr[voxel_param[e] + 1]++;
+      for (int p = 0; p < nparam; ++p) ptr[p + 1] += ptr[p];
+      std::vector<int> vox(std::max(ptr[nparam], 1));
+      std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+      for (long long e = 0; e < nv; ++e)
+        if (voxel_param[e] >= 0) vox[fill[voxel_param[e]]++] = (int)e;
+      const size_t need = (size_t)nparam + 1 + vox.size();
+      if (H->fmap_n < need) {
+        if (H->d_fmap) cudaFree(H->d_fmap);
+        H->d_fmap = nullptr;
+        H->fmap_n = 0;
+        CK(cudaMalloc(&H->d_fmap, need * sizeof(int)));
+        H->fmap_n = need;
+      }
+      CK(cudaMemcpyAsync(H->d_fmap, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice, H->stream));
+      CK(cudaMemcpyAsync(H->d_fmap + nparam + 1, vox.data(), vox.size() * sizeof(int), cudaMemcpyHostToDevice,
+                         H->stream));
+      CK(cudaStreamSynchronize(H->stream));   // host vectors go out of scope
+      H->fmap_key = key;
+      H->fmap_nparam = nparam;
+    }
+    Level& L0 = H->levels[0];
+    double W[21];
+    int t = 0;
+    for (int I = 0; I < 6; ++I)
+      for (int J = 0; J <= I; ++J) W[t++] = (I == J) ? dLdC[I * 6 + I] : dLdC[I * 6 + J] + dLdC[J * 6 + I];
+    CK(cudaMemcpyAsync(H->d_W, W, sizeof W, cudaMemcpyHostToDevice, H->stream));
+    EnergyArgs a{};
+    a.cells = L0.d_cells;
+    a.units = L0.all.d_nu;
+    a.chi = H->x64;
+    a.kc64 = H->kc64;
+    a.rho = H->rho_used;
+    a.ec = H->d_ec;
+    a.W = H->d_W;
+    // the voxel gradient and then the parameter sums, in the dead CG buffer q
+    // when they fit (18 x nvox FP64 or FP32 values), else in the staging buffer
+    const size_t qd = (size_t)18 * nv * (H->cfg.precision == FEMH_MIXED ? 4 : 8) / sizeof(double);
+    a.out = ((size_t)nv + nparam <= qd) ? grad_target(H, nullptr, 0) : stage(H, (size_t)nv + nparam);
+    a.ntot = L0.ntot;
+    a.k = H->hk;
+    a.law = make_law(H->cfg);
+    {
+      Prof prof_(H, "k_energy", 0.0);
+      k_energy<EN_GRAD><<<(unsigned)L0.all.nu.size(), 128, 0, H->stream>>>(a);
+      LAUNCH_CHECK(H);
+    }
+    double* pg = a.out + nv;
+    {
+      Prof prof_(H, "k_param_sum", 0.0);
+      k_param_sum<<<cdiv((long long)nparam * 32, 256), 256, 0, H->stream>>>(H->d_fmap, H->d_fmap + nparam + 1,
+                                                                           a.out, dLdrho_add, pg, nparam);
+      LAUNCH_CHECK(H);
+    }
+    to_host_or_dev(H, grad_out, pg, nparam, 0);
   });
 }
 

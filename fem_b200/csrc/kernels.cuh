@@ -887,6 +887,24 @@ __global__ void k_norm2(const CellDesc* cells, const NodeUnit* units, const TV* 
   if (threadIdx.x == 0) part[(long long)u.slot * kNumRhs + rhs] = acc[0];
 }
 
+// Field chain rule of fast_fem FEM3DFun::df (fast_fem/FEM3DFun.cpp:252-266)
+// for piecewise-constant fields: every voxel belongs to one field parameter
+// with weight 1, so grad[p] = sum over the voxels of p of (dL/drho_e + c).
+// One warp per parameter, its voxels in a fixed order (CSR built on the host):
+// deterministic, no atomics.
+__global__ void k_param_sum(const int* __restrict__ ptr, const int* __restrict__ vox,
+                            const double* __restrict__ dLdrho, double c, double* __restrict__ out, int nparam) {
+  const int p = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (p >= nparam) return;
+  double s = 0.0;
+  for (int q = ptr[p] + lane; q < ptr[p + 1]; q += 32) s += dLdrho[vox[q]] + c;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[p] = s;
+}
+
+
 __global__ void k_sum_slots(const int* slot_begin, const int* slot_end, const double* part, double* out,
                             int ncells) {
   FIN_PROLOGUE

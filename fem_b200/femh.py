@@ -32,7 +32,7 @@ EXPORTS = (
     "femh_config_default", "femh_create", "femh_destroy", "femh_homogenize", "femh_homogenize_grad",
     "femh_dCdrho", "femh_force_tensors", "femh_full_field", "femh_fluctuation", "femh_apply_operator", "femh_homogenize_batch",
     "femh_last_error", "femh_set_stream", "femh_kernel_launches", "femh_profile", "femh_profile_read",
-    "femh_energy_noalloc", "femh_batch_memory",
+    "femh_energy_noalloc", "femh_batch_memory", "femh_field_gradient",
 )
 
 
@@ -107,6 +107,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.femh_profile_read.argtypes = [vp, ctypes.POINTER(_KStat), ip, ctypes.POINTER(ctypes.c_int)]
     L.femh_energy_noalloc.argtypes = [ctypes.POINTER(_Config), ip, ip, ip, ctypes.c_double, vp, vp, vp, vp]
     L.femh_batch_memory.argtypes = [vp, ip, ctypes.POINTER(_Cell), dp, dp]
+    L.femh_field_gradient.argtypes = [vp, dp, ctypes.c_double, ip, ctypes.POINTER(ctypes.c_int), dp]
     _lib = L
     return L
 
@@ -248,6 +249,19 @@ class Engine:
             out = np.zeros(self.shape)
         self._check(self.lib.femh_homogenize_grad(self.h, dLdC.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                                   _ptr(out), _is_dev(out)))
+        return out
+
+    def field_grad(self, dLdC, voxel_param, nparam: int, add: float = 0.0) -> np.ndarray:
+        """Gradient w.r.t. the parameters of a piecewise-constant field
+        (femh_field_gradient): voxel_param[i, j, k] = the parameter of that
+        voxel (-1: none); ``add`` is added to dL/drho of every voxel."""
+        dLdC = np.ascontiguousarray(dLdC, dtype=np.float64).reshape(6, 6)
+        m = np.ascontiguousarray(voxel_param, dtype=np.int32).ravel()
+        out = np.zeros(nparam)
+        self._check(self.lib.femh_field_gradient(self.h, dLdC.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                 float(add), int(nparam),
+                                                 m.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out
 
     def dCdrho(self, out=None):

@@ -51,6 +51,15 @@ double PiecewiseConstant3D::f(const std::array<double, 3>& x) { return param[ind
 
 std::vector<SparseEntry> PiecewiseConstant3D::df(const std::array<double, 3>& x) { return {{index(x), 1.0}}; }
 
+bool PiecewiseConstant3D::voxelMap(const int n[3], std::vector<int>& map) const {
+  map.resize((size_t)n[0] * n[1] * n[2]);
+  for (int i = 0; i < n[0]; ++i)
+    for (int j = 0; j < n[1]; ++j)
+      for (int k = 0; k < n[2]; ++k)
+        map[((size_t)i * n[1] + j) * n[2] + k] = index({(i + 0.5) / n[0], (j + 0.5) / n[1], (k + 0.5) / n[2]});
+  return true;
+}
+
 // -------------------------------------------------------------------- FEM3DFun
 FEM3DFun::FEM3DFun() {}
 
@@ -106,13 +115,20 @@ double FEM3DFun::f() {
 std::vector<double> FEM3DFun::df() {
   const int nx = gridSize[0], ny = gridSize[1], nz = gridSize[2];
   const size_t nv = (size_t)nx * ny * nz;
-  std::vector<double> dfddist(nv, 0.0);
   double dLdC[36];
   for (int t = 0; t < 36; ++t) dLdC[t] = wG[t] * (G[t] - G0[t]);
-  check(h_, femh_homogenize_grad(h_, dLdC, dfddist.data(), 0));
   const double dm = (mw / (double)nv) * (density - m0);
-  for (auto& v : dfddist) v += dm;
   std::vector<double> grad(param.size(), 0.0);
+  std::vector<int> map;
+  if (!grad.empty() && field->voxelMap(gridSize.data(), map)) {   // chain rule on the device
+    for (int& p : map)
+      if (p < 0 || (size_t)p >= grad.size()) p = -1;
+    check(h_, femh_field_gradient(h_, dLdC, dm, (int)grad.size(), map.data(), grad.data()));
+    return grad;
+  }
+  std::vector<double> dfddist(nv, 0.0);
+  check(h_, femh_homogenize_grad(h_, dLdC, dfddist.data(), 0));
+  for (auto& v : dfddist) v += dm;
   for (int i = 0; i < nx; ++i)
     for (int j = 0; j < ny; ++j)
       for (int k = 0; k < nz; ++k) {

@@ -50,6 +50,11 @@ class RealField {
   virtual double f(const std::array<double, 3>& x) = 0;
   virtual std::vector<SparseEntry> df(const std::array<double, 3>& x) = 0;
   virtual void setParam(int i, double v) { param.at(i) = v; }
+  // For fields whose df at every voxel centre is one parameter with weight 1
+  // (piecewise-constant fields): that parameter per voxel of an n[0] x n[1] x
+  // n[2] grid, voxel (i*n1 + j)*n2 + k; false for other fields.  FEM3DFun::df
+  // then runs the field chain rule on the device (femh_field_gradient).
+  virtual bool voxelMap(const int n[3], std::vector<int>& map) const { (void)n; (void)map; return false; }
   virtual ~RealField() {}
 };
 
@@ -60,6 +65,7 @@ class PiecewiseConstant3D : public RealField {
   void allocate(int nx, int ny, int nz);
   double f(const std::array<double, 3>& x) override;
   std::vector<SparseEntry> df(const std::array<double, 3>& x) override;
+  bool voxelMap(const int n[3], std::vector<int>& map) const override;
 
  private:
   int index(const std::array<double, 3>& x) const;

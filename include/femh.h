@@ -143,6 +143,21 @@ femh_status femh_homogenize(femh_handle* h, int nx, int ny, int nz, double hvox,
 femh_status femh_homogenize_grad(femh_handle* h, const double dLdC[36], double* dLdrho,
                                  int out_on_device);
 
+/* Gradient of a loss with respect to the parameters of a piecewise-constant
+ * density field, at the last solve: the field chain rule of FEM3DFun::df
+ * (fast_fem/FEM3DFun.cpp:252-266) for the fields whose df(x) is one parameter
+ * with weight 1 (PiecewiseConstant3D / Sym3D / Cubic3D,
+ * fast_fem/PiecewiseConstant*3D.cpp), on the device:
+ *   grad[p] = sum over voxels e with voxel_param[e] == p of (dL/drho_e + dLdrho_add),
+ * dL/drho_e as femh_homogenize_grad computes it from dLdC, dLdrho_add a term
+ * added to every voxel (FEM3DFun's density penalty, mw/n (density - m0),
+ * FEM3DFun.cpp:229-231).  voxel_param: nx*ny*nz host ints in [0, nparam), or
+ * -1 for a voxel that belongs to no parameter; grad_out: nparam host doubles.
+ * The sums run in a fixed order (bit-reproducible).  The voxel lists are built
+ * on the host and kept on the device until the map or the cells change. */
+femh_status femh_field_gradient(femh_handle* h, const double dLdC[36], double dLdrho_add, int nparam,
+                                const int* voxel_param, double* grad_out);
+
 /* dC^H_IJ/drho_e for the 21 lower-triangle pairs, layout [21][nx*ny*nz]. */
 femh_status femh_dCdrho(femh_handle* h, double* out, int out_on_device);
 

@@ -1,4 +1,4 @@
-// A stand-in for libfemh's C ABI (test double, no GPU): the nine entry points
+// A stand-in for libfemh's C ABI (test double, no GPU): the ten entry points
 // the C++ host layer calls, returning deterministic tensors so that the host
 // layer's own logic -- material mapping, repMaterialAssignment, parameter
 // formulas, batch bookkeeping, error paths -- can be checked on the CPU.
@@ -126,6 +126,18 @@ femh_status femh_homogenize_grad(femh_handle* h, const double dLdC[36], double* 
   double t = 0.0;
   for (int a = 0; a < 6; ++a) t += dLdC[7 * a];
   for (int i = 0; i < h->nvox; ++i) dLdrho[i] = t;
+  return FEMH_OK;
+}
+
+// grad[p] = sum over the voxels of p of (trace(dL/dC) + add)
+femh_status femh_field_gradient(femh_handle* h, const double dLdC[36], double add, int nparam, const int* map,
+                                double* grad) {
+  if (!h || !dLdC || !map || !grad || nparam < 1 || h->nvox < 1) return FEMH_E_STATE;
+  double t = 0.0;
+  for (int a = 0; a < 6; ++a) t += dLdC[7 * a];
+  for (int p = 0; p < nparam; ++p) grad[p] = 0.0;
+  for (int e = 0; e < h->nvox; ++e)
+    if (map[e] >= 0) grad[map[e]] += t + add;
   return FEMH_OK;
 }
 

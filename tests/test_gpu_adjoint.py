@@ -64,3 +64,32 @@ def test_torch_autograd_gradcheck(femh):
     def f(r):
         return (homogenize(r, eng) * W).sum()
     assert torch.autograd.gradcheck(f, (rho,), eps=1e-6, atol=1e-7, rtol=1e-5)
+
+
+def test_field_chain_rule_on_device(femh):
+    """femh_field_gradient: the field chain rule of FEM3DFun::df
+    (fast_fem/FEM3DFun.cpp:252-266) for a piecewise-constant field, on the
+    device -- equal to the per-voxel adjoint gradient summed over each
+    parameter's voxels (plus the per-voxel density term), bit-identical
+    across calls; voxels mapped to -1 contribute nothing; a parameter index out
+    of range is an argument error."""
+    from fem_b200 import fields
+    rho = fields.smooth_cell(16, 2.0, seed=21)
+    e = femh.Engine()
+    C, _ = e.homogenize(rho)
+    dLdC = 2.0 * (C - np.diag([0.1] * 3 + [0.03] * 3))
+    g = e.grad(dLdC)
+    i, j, k = np.meshgrid(*(np.arange(16) // 4,) * 3, indexing="ij")
+    vp = (i * 4 + j) * 4 + k
+    gp = e.field_grad(dLdC, vp, 64, add=0.01)
+    want = (g + 0.01).reshape(4, 4, 4, 4, 4, 4).sum(axis=(1, 3, 5)).ravel()
+    assert np.abs(gp - want).max() < 1e-12 * np.abs(want).max()
+    assert np.array_equal(gp, e.field_grad(dLdC, vp, 64, add=0.01))
+    vp2 = vp.copy()
+    vp2[:, :, :8] = -1
+    want2 = np.bincount(vp2[vp2 >= 0].ravel(), weights=(g + 0.01)[vp2 >= 0].ravel(), minlength=64)
+    assert np.abs(e.field_grad(dLdC, vp2, 64, add=0.01) - want2).max() < 1e-12 * np.abs(want2).max()
+    vp2[0, 0, 0] = 64
+    with pytest.raises(femh.FemhError) as ex:
+        e.field_grad(dLdC, vp2, 64)
+    assert ex.value.code == femh.FEMH_E_ARG
