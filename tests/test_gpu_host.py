@@ -124,9 +124,11 @@ def test_force_driven_coarsening_matches_reference_code(host_out):
     NumericalCoarsening (SamplesGenerator/NumericalCoarsening.cpp:266-340, built
     as shipped -- float, 1 + 1e-5 diagonal scaling -- with Eigen's LU for the
     absent PARDISO) on structure 0 subdivided to 8^3: the 21 tensor values and
-    (rho, Y, nu_xy, G) within 1e-4 relative (the engine returns the exact,
-    unscaled values; the reference's scaling and float arithmetic move them by
-    less than that)."""
+    (rho, Y, nu_xy, G): tensor within 1e-4, parameters within 3e-4 relative.
+    The engine returns the exact, unscaled values; the reference's 1 + 1e-5
+    diagonal scaling moves Y on this cell by 1.2e-4 (the scaled restatement
+    matches the reference to 2e-5, tests/test_ref_pins.py), its float
+    arithmetic by ~1e-6."""
     from oracle import ref as R
     if not R.available("libnc_ref.so"):
         pytest.skip("oracle/_ref/libnc_ref.so not built")
@@ -137,4 +139,4 @@ def test_force_driven_coarsening_matches_reference_code(host_out):
     nu = lame[1][1] / (2 * (lame[1][1] + lame[1][0]))
     tv, pv = R.nc_coarsen(cells, E, nu, (0.0, 1.0), R.CUBIC)
     assert np.abs(np.array(host_out["force_tensors"])[:21] - tv).max() < 1e-4 * np.abs(tv).max()
-    assert np.abs(np.array(host_out["force_params"])[:4] - pv).max() < 1e-4 * np.abs(pv).max()
+    assert np.abs(np.array(host_out["force_params"])[:4] - pv).max() < 3e-4 * np.abs(pv).max()
