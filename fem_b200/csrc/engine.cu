@@ -408,6 +408,7 @@ struct femh_handle {
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int wait_limit = kWaitLimit;   // try_wait rounds of the staged kernels' stage waits
+  int* d_loop = nullptr;         // CG iterations run on the device in the current solve (WHILE-node count)
   int* d_err = nullptr;   // [0] set by a stencil kernel whose bounded wait ran out,
                           // [1] by k_coef on a NaN, infinite or negative density
 
@@ -1642,31 +1643,63 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
     }
   }
   const int chunk = H->prof ? 1 : std::max(1, c.graph_chunk > 0 ? c.graph_chunk : 8);
+  // The iterations run on the device without the host: a CUDA graph whose
+  // WHILE node repeats `chunk` captured iterations while k_while_cond finds
+  // live cells (and, for a batch, more than half of the listed ones); the host
+  // wakes only to compact a batch's unit lists or at the end.
   cudaGraphExec_t exec = nullptr;
-  long long graph_kernels = 0;
+  long long graph_kernels = 0;   // kernels of one pass of the loop body
+  int listed = nc;               // cells covered by the current unit lists
+  const int limit = max_iter + chunk;
+  CK(cudaMemsetAsync(H->d_loop, 0, sizeof(int), s));
   auto capture = [&]() {
     if (!(c.graph_chunk > 0 && !H->prof)) return;
     cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle cond;
+    cudaGraph_t body = nullptr;
+    try {
+      CK(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = cond;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node;
+      CK(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+      body = cp.conditional.phGraph_out[0];
+    } catch (...) {
+      cudaGraphDestroy(g);
+      throw;
+    }
     H->capturing = true;
     H->cap_count = 0;
-    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     try {
       for (int i = 0; i < chunk; ++i) pcg_iteration<PR>(H, kcg);
+      k_while_cond<<<1, 1024, 0, s>>>(cond, H->d_state, nc, listed, H->d_loop, chunk, limit);
+      LAUNCH_CHECK(H);
     } catch (...) {
       H->capturing = false;
-      cudaStreamEndCapture(s, &g);
-      if (g) cudaGraphDestroy(g);
+      cudaGraph_t tmp = nullptr;
+      cudaStreamEndCapture(s, &tmp);
+      cudaGraphDestroy(g);
       throw;
     }
     H->capturing = false;
     graph_kernels = H->cap_count;
-    CK(cudaStreamEndCapture(s, &g));
-    CK(cudaGraphInstantiate(&exec, g, 0));
+    cudaGraph_t got = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(s, &got);
+    if (ee != cudaSuccess) {
+      cudaGraphDestroy(g);
+      CK(ee);
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
     cudaGraphDestroy(g);
+    CK(ei);
   };
   // batch compaction bookkeeping
   std::vector<FullLists> full;
-  int listed = nc;   // cells covered by the current unit lists
   auto restore = [&]() {
     if (full.empty()) return;
     for (size_t l = 0; l < H->levels.size(); ++l) set_units(H, H->levels[l], full[l], nullptr);
@@ -1677,14 +1710,19 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
   try {
     while (true) {
       if (exec) {
+        int loop_now = done;
         CK(cudaGraphLaunch(exec, s));
-        H->launches += graph_kernels;
+        CK(cudaMemcpyAsync(&loop_now, H->d_loop, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(H->state.data(), stt, sizeof(CGState) * H->state.size(), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        H->launches += graph_kernels * (long long)std::max(1, (loop_now - done) / chunk);
+        done = loop_now;
       } else {
         for (int i = 0; i < chunk; ++i) pcg_iteration<PR>(H, kcg);
+        done += chunk;
+        CK(cudaMemcpyAsync(H->state.data(), stt, sizeof(CGState) * H->state.size(), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
       }
-      done += chunk;
-      CK(cudaMemcpyAsync(H->state.data(), stt, sizeof(CGState) * H->state.size(), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
       prof_resolve(H);
       std::vector<char> keep(nc, 0);
       int alive = 0;
@@ -2072,6 +2110,7 @@ femh_status femh_create(femh_handle** out, const femh_config* cfg) {
     CK(cudaMemcpy(H->d_K0, H->K0, sizeof(double) * 576, cudaMemcpyHostToDevice));
     H->d_err = H->perm.arr<int>(2);
     CK(cudaMemset(H->d_err, 0, 2 * sizeof(int)));
+    H->d_loop = H->perm.arr<int>(1);
     // FEMH_STAGE_WAIT_LIMIT (tests only): fewer try_wait rounds per stage wait
     // of the bulk-copy staged kernels, so that a wait runs out although its
     // copies complete -- the kernel then drains them with the full limit, flags

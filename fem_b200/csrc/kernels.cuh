@@ -887,6 +887,34 @@ __global__ void k_norm2(const CellDesc* cells, const NodeUnit* units, const TV* 
   if (threadIdx.x == 0) part[(long long)u.slot * kNumRhs + rhs] = acc[0];
 }
 
+// Condition of the CUDA-graph WHILE node around the captured CG iterations
+// (one CTA): another pass of `chunk` iterations while some listed cell still
+// iterates, the iteration budget `limit` is not spent, and -- for a batch --
+// more than half of the `listed` cells still iterate (otherwise the host
+// compacts the unit lists to the live cells and relaunches).  loop[0] counts
+// the iterations run in this solve, so the loop always ends.
+__global__ void k_while_cond(cudaGraphConditionalHandle h, const CGState* __restrict__ stt, int ncells,
+                             int listed, int* loop, int chunk, int limit) {
+  __shared__ int alive;
+  if (threadIdx.x == 0) alive = 0;
+  __syncthreads();
+  int mine = 0;
+  for (int c = threadIdx.x; c < ncells; c += blockDim.x) {
+    bool a = false;
+#pragma unroll
+    for (int r = 0; r < kNumRhs; ++r) a = a || stt[c * kNumRhs + r].active != 0;
+    mine += a ? 1 : 0;
+  }
+  if (mine) atomicAdd(&alive, mine);   // integer count: exact in any order
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int done = loop[0] + chunk;
+    loop[0] = done;
+    const bool more = alive > 0 && done <= limit && !(ncells > 1 && 2 * alive <= listed);
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+  }
+}
+
 // Field chain rule of fast_fem FEM3DFun::df (fast_fem/FEM3DFun.cpp:252-266)
 // for piecewise-constant fields: every voxel belongs to one field parameter
 // with weight 1, so grad[p] = sum over the voxels of p of (dL/drho_e + c).
