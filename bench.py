@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--batch-cells", type=int, default=4096, help="cells of the uneven batch leg")
     ap.add_argument("--no-autotune", action="store_true",
                     help="heuristic tile shapes (the first stencil launches are then the solve's own)")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="plain launches instead of the CUDA-graph loop (ncu cannot profile kernels inside a "
+                         "graph with conditional nodes): the launch-list command")
     ap.add_argument("--quick", action="store_true",
                     help="timed device steps only (no e2e / FP64 / roofline / CPU legs): the profiling command")
     return ap.parse_args()
@@ -240,7 +243,8 @@ def main():
     Ct = target_tensor(n)
 
     stream = torch.cuda.current_stream()
-    cfg = F.Config(device=local, precision=F.MIXED_PC, solver=F.GMG_PCG, autotune=0 if args.no_autotune else 1)
+    cfg = F.Config(device=local, precision=F.MIXED_PC, solver=F.GMG_PCG, autotune=0 if args.no_autotune else 1,
+                   graph_chunk=0 if args.no_graphs else 8)
     eng = F.Engine(cfg)
     eng.set_stream(stream.cuda_stream)
     rho_d = torch.from_numpy(rho_h).cuda()

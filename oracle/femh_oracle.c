@@ -13,8 +13,8 @@
  *     closed form matlab/homogenize.m:121-167 is the same matrix).  Node order
  *     is the z-fastest `oneV` order of fast_fem/FEM3DFun.cpp:58-60
  *     (a = 4*ax + 2*ay + az), DOF 3*a + c.
- *   - per-voxel coefficient: SIMP E_min + rho^p (E_s - E_min) (BASELINE
- *     material law; MaterialOpt/src/FEM3DFun.cpp:244-257 is the same form),
+ *   - per-voxel coefficient: SIMP E_min + rho^p (E_s - E_min)
+ *     (MaterialOpt/src/FEM3DFun.cpp:244-257),
  *     x/(3-2x) (fast_fem/FEM3DFun.cpp:20-27) and the two-material coefficient
  *     {hi, lo} (SamplesGenerator/NumericalCoarseningUsingMultiGrid.cpp:235-241).
  *   - periodic six-load-case problem: total displacement u^I = eps^I x + chi^I

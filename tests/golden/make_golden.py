@@ -8,6 +8,7 @@ and writes the dense matrix, one row per line.  It needs the reference tree
 and is run by hand; the committed output is what the tests read.
 
 usage: python tests/golden/make_golden.py <path-to-reference-tree>
+       (or set FEMH_REFERENCE_TREE)
 """
 import os
 import sys
@@ -31,4 +32,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    tree = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FEMH_REFERENCE_TREE")
+    if not tree:
+        sys.exit("usage: make_golden.py <path-to-reference-tree>  (or set FEMH_REFERENCE_TREE)")
+    main(tree)
