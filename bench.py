@@ -175,45 +175,56 @@ def cpu_baseline(rho, Ct):
 
 
 # ----------------------------------------------------- uneven batch leg --
-def batched_uneven(F, local: int, ncell: int, fp64_sample: int = 128) -> dict:
+def batched_uneven(F, local: int, ncell: int, world: int = 1, rank: int = 0, fp64_sample: int = 128) -> dict:
     """The seeded uneven set (n in {16,24,32,48,64}, binary voxels, volume
     fraction U[0.2,0.6]) solved in mixed precision in as few batched calls as
-    fit the device (one for the 4096 cells), with dC^H/drho contracted against
-    a fixed weight tensor per cell (the adjoint pass), against solving cells
-    one at a time with the plain FP64 path (set-up included, timed on the
-    first `fp64_sample` cells).  Wall time around the calls (each call ends
-    with its results on the host)."""
+    fit the device (one for the 4096 cells on one B200), with dC^H/drho
+    contracted against a fixed weight tensor per cell (the adjoint pass),
+    against solving cells one at a time with the plain FP64 path (set-up
+    included, timed on the first `fp64_sample` cells, rank 0).  With several
+    ranks the cells are sharded by voxels (fem_b200.dist.shard, no data-path
+    collective) and the time is the max over ranks.  Wall time around the calls
+    (each call ends with its results on the host)."""
     from fem_b200 import fields
+    from fem_b200.dist import max_over_ranks, shard
     cells = fields.uneven_batch(4096, seed=7, count=ncell)
-    W = np.tile(np.diag([1.0, 1.0, 1.0, 0.5, 0.5, 0.5]), (len(cells), 1, 1))
+    mine = shard([float(c.size) for c in cells], world)[rank]
+    my_cells = [cells[i] for i in mine]
+    W = np.tile(np.diag([1.0, 1.0, 1.0, 0.5, 0.5, 0.5]), (len(my_cells), 1, 1))
     e = F.Engine(F.Config(device=local, precision=F.MIXED_PC))
-    need, avail = e.batch_memory([c.shape for c in cells])
-    e.batch(cells[:8], dLdC=W[:8], allow_unconverged=True)   # warm-up: library, autotuner code paths
+    need, avail = e.batch_memory([c.shape for c in my_cells])
+    e.batch(my_cells[:8], dLdC=W[:8], allow_unconverged=True)   # warm-up: library, autotuner code paths
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
     t0 = time.perf_counter()
-    C, infos, grads = e.batch(cells, dLdC=W, allow_unconverged=True)
-    t_batch = time.perf_counter() - t0
+    C, infos, grads = e.batch(my_cells, dLdC=W, allow_unconverged=True)
+    t_batch = max_over_ranks(time.perf_counter() - t0, device="cuda")
     e.close()
     its = np.array([max(i["iterations"]) for i in infos])
-    bad = sum(1 for i in infos if i["status"] != 0)
-    e64 = F.Engine(F.Config(device=local, precision=F.FP64))
-    k = min(fp64_sample, len(cells))
-    e64.homogenize(cells[0])
-    t0 = time.perf_counter()
-    for c in cells[:k]:
-        C1, _ = e64.homogenize(c, allow_unconverged=True)
-        e64.grad(np.diag([1.0, 1.0, 1.0, 0.5, 0.5, 0.5]))
-    t_one = (time.perf_counter() - t0) / k
-    e64.close()
-    vox = sum(c.size for c in cells)
-    return {"cells": len(cells), "voxels": int(vox), "cells_per_s": len(cells) / t_batch, "seconds": t_batch,
-            "calls": int(max(1, np.ceil(sum(need) / (0.92 * avail)))), "device_bytes_needed": float(sum(need)),
-            "iterations_p50_p90_max": [int(np.percentile(its, 50)), int(np.percentile(its, 90)), int(its.max())],
-            "not_converged": bad,
-            "fp64_one_at_a_time_cells_per_s": 1.0 / t_one,
-            "fp64_sample": f"first {k} cells of the set, one femh_homogenize + femh_homogenize_grad each",
-            "speedup_vs_fp64_one_at_a_time": (len(cells) / t_batch) * t_one,
-            "precision": "FP64 CG + FP32 multigrid, gradients contracted with a fixed dL/dC",
-            "set": "fields.uneven_batch(4096, seed=7)"}
+    bad = int(max_over_ranks(sum(1 for i in infos if i["status"] != 0), device="cuda"))
+    out = {"cells": len(cells), "voxels": int(sum(c.size for c in cells)), "ranks": world,
+           "cells_per_s": len(cells) / t_batch, "seconds": t_batch,
+           "calls_per_rank": int(max(1, np.ceil(sum(need) / (0.92 * avail)))),
+           "device_bytes_needed_rank0": float(sum(need)),
+           "iterations_p50_p90_max_rank0": [int(np.percentile(its, 50)), int(np.percentile(its, 90)), int(its.max())],
+           "not_converged_max_over_ranks": bad,
+           "precision": "FP64 CG + FP32 multigrid, gradients contracted with a fixed dL/dC",
+           "set": "fields.uneven_batch(4096, seed=7)"}
+    if rank == 0:
+        e64 = F.Engine(F.Config(device=local, precision=F.FP64))
+        k = min(fp64_sample, len(cells))
+        e64.homogenize(cells[0])
+        t0 = time.perf_counter()
+        for c in cells[:k]:
+            e64.homogenize(c, allow_unconverged=True)
+            e64.grad(np.diag([1.0, 1.0, 1.0, 0.5, 0.5, 0.5]))
+        t_one = (time.perf_counter() - t0) / k
+        e64.close()
+        out.update({"fp64_one_at_a_time_cells_per_s_one_gpu": 1.0 / t_one,
+                    "fp64_sample": f"first {k} cells of the set, one femh_homogenize + femh_homogenize_grad each",
+                    "speedup_per_gpu_vs_fp64_one_at_a_time": (len(cells) / t_batch / world) * t_one})
+    return out
 
 
 # ----------------------------------------------------------------- main ---
@@ -378,8 +389,8 @@ def main():
     }
     eng.close()
     eng64.close()
-    if not args.no_batch and world == 1:
-        out["batched_uneven"] = batched_uneven(F, local, args.batch_cells)
+    if not args.no_batch:
+        out["batched_uneven"] = batched_uneven(F, local, args.batch_cells, world, rank)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(rho_h, Ct)
     if rank == 0:
