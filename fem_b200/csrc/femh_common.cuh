@@ -67,7 +67,13 @@ struct CGState {
   double tol;
   int outer;        // defect correction: this (cell, rhs) takes part in the current outer step
   int fallback;     // 1: the multigrid preconditioner turned indefinite; Jacobi from then on
+  double best;      // smallest relative residual so far (inner solves of defect correction)
+  int since;        // iterations since it last halved
 };
+// An inner (FP32) solve of defect correction stops when its residual has not
+// halved for this many iterations: it has reached what its arithmetic resolves,
+// and the next outer step (FP64 residual) continues from there.
+constexpr int kInnerStallWindow = 200;
 enum CGStatus : int { CG_RUNNING = 0, CG_CONVERGED = 1, CG_MAXITER = 2, CG_BREAKDOWN = 3 };
 
 template <typename T> struct VT { using type = T; };

@@ -297,6 +297,8 @@ __global__ void k_fin_init(CGState* stt, const int* slot_begin, const int* slot_
   S.rz = jacobi ? sum_slots(part, slot_begin[cell], slot_end[cell], rhs, 2, 1) : 0.0;
   S.iters = 0;
   S.rel = (S.bnorm2 > 0.0) ? sqrt(rr / S.bnorm2) : 0.0;
+  S.best = S.rel;
+  S.since = 0;
   if (!(S.bnorm2 > 0.0) || !(rr > 0.0) || S.rel < S.tol) { S.active = 0; S.status = CG_CONVERGED; }
   if (lead) stt[t] = S;
 }
@@ -364,6 +366,10 @@ __global__ void k_fin_beta(CGState* stt, const int* slot_begin, const int* slot_
     S.status = CG_CONVERGED;
   } else if (S.iters >= S.max_iter) {
     S.active = 0;
+    S.status = CG_MAXITER;
+  } else if (S.outer && (S.rel < 0.5 * S.best ? (S.best = S.rel, S.since = 0, false)
+                                               : ++S.since >= kInnerStallWindow)) {
+    S.active = 0;   // inner solve at its arithmetic's floor: hand back to the outer step
     S.status = CG_MAXITER;
   } else if (!isfinite(rzn) || !(rzn > 0.0)) {
     if (!jacobi && !S.fallback && isfinite(rz_jac) && rz_jac > 0.0) {
