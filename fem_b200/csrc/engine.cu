@@ -2111,13 +2111,12 @@ femh_status femh_create(femh_handle** out, const femh_config* cfg) {
     H->d_err = H->perm.arr<int>(2);
     CK(cudaMemset(H->d_err, 0, 2 * sizeof(int)));
     H->d_loop = H->perm.arr<int>(1);
-    // FEMH_STAGE_WAIT_LIMIT (tests only): fewer try_wait rounds per stage wait
-    // of the bulk-copy staged kernels, so that a wait runs out although its
-    // copies complete -- the kernel then drains them with the full limit, flags
-    // the handle and returns, and the call reports FEMH_E_CUDA
+    // FEMH_STAGE_WAIT_LIMIT=0 (tests only): a stage wait of the bulk-copy staged
+    // kernels that is not met at its first try gives up, although its copies
+    // complete -- the kernel then drains them with the full limit, flags the
+    // handle and returns, and the call reports FEMH_E_CUDA
     if (const char* w = std::getenv("FEMH_STAGE_WAIT_LIMIT")) {
-      const long v = std::strtol(w, nullptr, 10);
-      if (v >= 0 && v < kWaitLimit) H->wait_limit = (int)v;
+      if (std::strtol(w, nullptr, 10) == 0) H->wait_limit = 0;
     }
     // FEMH_ARENA_LIMIT_BYTES (tests only): the handle's set-up allocations fail
     // with FEMH_E_OOM beyond this many bytes, as on a device without room

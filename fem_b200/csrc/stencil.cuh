@@ -50,7 +50,7 @@ struct StencilArgs {
   double omega;
   float2 kp[8];          // FP32 pairs (x = y) of A, Bd-Bo, Bo, D1-O1, O1, D2-O2, O2, G
   int* err;              // set non-zero by a kernel whose bounded wait ran out
-  int wait_limit;        // try_wait rounds of a stage wait (kWaitLimit; smaller only in tests)
+  int wait_limit;        // 0: a stage wait not met at its first try gives up (tests); else kWaitLimit rounds
 };
 
 template <typename T>
@@ -1241,6 +1241,16 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int lim
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
+// Stage wait of the staged kernels: the compile-time bound above, except that
+// a wait that does not succeed at its first try gives up at once when
+// give_up_early is set (FEMH_STAGE_WAIT_LIMIT=0, tests of the timeout path).
+// The flag is read only on that slow path, so it costs no register in the
+// kernels, which run at their register cap.
+__device__ __forceinline__ bool mbar_wait_stage(unsigned bar, unsigned parity, int give_up_early) {
+  if (mbar_try_wait(bar, parity)) return true;
+  if (give_up_early) return false;
+  return mbar_wait(bar, parity);
+}
 __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                "l"(src), "r"(bytes), "r"(bar)
@@ -1365,7 +1375,7 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
     for (int g = 0; g < kBulkSlots && g < G; ++g) issue(g);
   int waited = 0;   // stages 0 .. waited-1 completed for this thread (the exit drain starts there)
   auto wait_stage = [&](int g) {
-    if (!mbar_wait(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1), a.wait_limit)) {
+    if (!mbar_wait_stage(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1), a.wait_limit == 0)) {
       if (a.err) atomicExch(a.err, 1);
       abort_flag = 1;
     } else if (waited == g) {
@@ -1673,7 +1683,7 @@ stencil1b_kernel(StencilArgs<TIn, double, double, double> a) {
     for (int g = 0; g < kBulkSlots && g < G; ++g) issue(g);
   int waited = 0;   // stages 0 .. waited-1 completed for this thread (the exit drain starts there)
   auto wait_stage = [&](int g) {
-    if (!mbar_wait(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1), a.wait_limit)) {
+    if (!mbar_wait_stage(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1), a.wait_limit == 0)) {
       if (a.err) atomicExch(a.err, 1);
       abort_flag = 1;
     } else if (waited == g) {
