@@ -2111,10 +2111,10 @@ femh_status femh_create(femh_handle** out, const femh_config* cfg) {
     H->d_err = H->perm.arr<int>(2);
     CK(cudaMemset(H->d_err, 0, 2 * sizeof(int)));
     H->d_loop = H->perm.arr<int>(1);
-    // FEMH_STAGE_WAIT_LIMIT=0 (tests only): a stage wait of the bulk-copy staged
-    // kernels that is not met at its first try gives up, although its copies
-    // complete -- the kernel then drains them with the full limit, flags the
-    // handle and returns, and the call reports FEMH_E_CUDA
+    // FEMH_STAGE_WAIT_LIMIT=0 (tests only): every stage wait of the bulk-copy
+    // staged kernels gives up at once, although its copies complete -- the
+    // kernel then drains them with the full limit, flags the handle and
+    // returns, and the call reports FEMH_E_CUDA
     if (const char* w = std::getenv("FEMH_STAGE_WAIT_LIMIT")) {
       if (std::strtol(w, nullptr, 10) == 0) H->wait_limit = 0;
     }

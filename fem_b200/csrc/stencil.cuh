@@ -50,7 +50,7 @@ struct StencilArgs {
   double omega;
   float2 kp[8];          // FP32 pairs (x = y) of A, Bd-Bo, Bo, D1-O1, O1, D2-O2, O2, G
   int* err;              // set non-zero by a kernel whose bounded wait ran out
-  int wait_limit;        // 0: a stage wait not met at its first try gives up (tests); else kWaitLimit rounds
+  int wait_limit;        // 0: every stage wait gives up at once (tests); else kWaitLimit rounds
 };
 
 template <typename T>
@@ -1242,13 +1242,12 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int lim
   return false;
 }
 // Stage wait of the staged kernels: the compile-time bound above, except that
-// a wait that does not succeed at its first try gives up at once when
-// give_up_early is set (FEMH_STAGE_WAIT_LIMIT=0, tests of the timeout path).
-// The flag is read only on that slow path, so it costs no register in the
-// kernels, which run at their register cap.
-__device__ __forceinline__ bool mbar_wait_stage(unsigned bar, unsigned parity, int give_up_early) {
-  if (mbar_try_wait(bar, parity)) return true;
-  if (give_up_early) return false;
+// every wait gives up at once when give_up (FEMH_STAGE_WAIT_LIMIT=0, tests of
+// the timeout path) is set.  A flag test rather than a runtime round limit:
+// the kernels run at their register cap, and a runtime loop bound made the
+// FP64 one spill.
+__device__ __forceinline__ bool mbar_wait_stage(unsigned bar, unsigned parity, int give_up) {
+  if (give_up) return false;
   return mbar_wait(bar, parity);
 }
 __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
