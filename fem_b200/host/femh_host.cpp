@@ -60,6 +60,51 @@ bool PiecewiseConstant3D::voxelMap(const int n[3], std::vector<int>& map) const 
   return true;
 }
 
+// ------------------------------------------- PiecewiseConstantSym3D / Cubic3D
+void PiecewiseConstantSym3D::allocate(int nx, int ny, int nz) {
+  gridSize[0] = nx;
+  gridSize[1] = ny;
+  gridSize[2] = nz;
+  param.assign((size_t)nx * ny * nz, 1.0);
+}
+
+namespace {
+double reflect(double c) {
+  c *= 2.0;
+  return c > 1.0 ? 2.0 - c : c;
+}
+int cell_of(double c, int n) { return std::min(std::max((int)(c * n), 0), n - 1); }
+}  // namespace
+
+int PiecewiseConstantSym3D::index(const std::array<double, 3>& x) const {
+  int idx[3];
+  for (int d = 0; d < 3; ++d) idx[d] = cell_of(reflect(x[d]), gridSize[d]);
+  return (idx[0] * gridSize[1] + idx[1]) * gridSize[2] + idx[2];
+}
+
+int PiecewiseConstantCubic3D::index(const std::array<double, 3>& x) const {
+  double c[3] = {reflect(x[0]), reflect(x[1]), reflect(x[2])};
+  if (c[0] < c[1]) std::swap(c[0], c[1]);   // x >= y >= z
+  if (c[0] < c[2]) std::swap(c[0], c[2]);
+  if (c[1] < c[2]) std::swap(c[1], c[2]);
+  int idx[3];
+  for (int d = 0; d < 3; ++d) idx[d] = cell_of(c[d], gridSize[d]);
+  return (idx[0] * gridSize[1] + idx[1]) * gridSize[2] + idx[2];
+}
+
+double PiecewiseConstantSym3D::f(const std::array<double, 3>& x) { return param[index(x)]; }
+
+std::vector<SparseEntry> PiecewiseConstantSym3D::df(const std::array<double, 3>& x) { return {{index(x), 1.0}}; }
+
+bool PiecewiseConstantSym3D::voxelMap(const int n[3], std::vector<int>& map) const {
+  map.resize((size_t)n[0] * n[1] * n[2]);
+  for (int i = 0; i < n[0]; ++i)
+    for (int j = 0; j < n[1]; ++j)
+      for (int k = 0; k < n[2]; ++k)
+        map[((size_t)i * n[1] + j) * n[2] + k] = index({(i + 0.5) / n[0], (j + 0.5) / n[1], (k + 0.5) / n[2]});
+  return true;
+}
+
 // -------------------------------------------------------------------- FEM3DFun
 FEM3DFun::FEM3DFun() {}
 

@@ -71,6 +71,31 @@ class PiecewiseConstant3D : public RealField {
   int index(const std::array<double, 3>& x) const;
 };
 
+// Mirror-symmetric field (fast_fem/PiecewiseConstantSym3D.cpp): every
+// coordinate in [0, 1] is reflected into the lower half (c -> 2c, then 2 - 2c
+// above 1) and mapped onto an nx x ny x nz parameter grid -- the parameters of
+// one octant, mirrored into the other seven.
+class PiecewiseConstantSym3D : public RealField {
+ public:
+  int gridSize[3] = {0, 0, 0};
+  void allocate(int nx, int ny, int nz);
+  double f(const std::array<double, 3>& x) override;
+  std::vector<SparseEntry> df(const std::array<double, 3>& x) override;
+  bool voxelMap(const int n[3], std::vector<int>& map) const override;
+
+ protected:
+  virtual int index(const std::array<double, 3>& x) const;
+};
+
+// Cubic-symmetric field (fast_fem/PiecewiseConstantCubic3D.cpp, the field of
+// fast_fem/run3d.cpp:176-182): reflected as the mirror-symmetric field, then
+// the three coordinates sorted so that x >= y >= z (the 48 symmetries of the
+// cube map onto one parameter).
+class PiecewiseConstantCubic3D : public PiecewiseConstantSym3D {
+ protected:
+  int index(const std::array<double, 3>& x) const override;
+};
+
 // Homogenized-stiffness objective on a periodic voxel cell.  G is C^H (both
 // triangles); f = 0.5 sum wG (G-G0)^2 + 0.5 mw (density-m0)^2; df is the
 // adjoint gradient w.r.t. the field parameters.

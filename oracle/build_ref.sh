@@ -13,7 +13,8 @@
 #       tree, is replaced by oracle/ref_shim/pardiso_eigen.cpp (the
 #       reference's vendored Eigen sparse LU).
 #   oracle/_ref/libfastfem_ref.so fast_fem's FEM3DFun (setParam's energy loop,
-#       f, df and the field chain rule) and PiecewiseConstant3D, entry
+#       f, df and the field chain rule) and the PiecewiseConstant{,Sym,Cubic}3D
+#       fields, entry
 #       oracle/ref_fastfem.cpp; topoOptLib, absent from the tree, is replaced
 #       by the stand-in headers of oracle/ref_shim/ whose Homogenize() runs the
 #       oracle's FP64 solve.
@@ -69,7 +70,8 @@ if [ -f "$HERE/ref_fastfem.cpp" ] && { [ ! -f "$FF" ] || [ "$HERE/ref_fastfem.cp
   g++ $COMMON -O2 -shared -I"$HERE/ref_shim" -I"$HERE" -I"$REF/fast_fem" -I"$REF/femlib/include" \
       -Wl,--no-undefined -o "$FF" "$HERE/ref_fastfem.cpp" "$REF/fast_fem/FEM3DFun.cpp" \
       "$REF/fast_fem/ArrayUtil.cpp" "$REF/fast_fem/PiecewiseConstant3D.cpp" \
-      "$REF/fast_fem/PiecewiseConstantCubic3D.cpp" "$REF/fast_fem/RealFun.cpp" \
+      "$REF/fast_fem/PiecewiseConstantCubic3D.cpp" "$REF/fast_fem/PiecewiseConstantSym3D.cpp" \
+      "$REF/fast_fem/RealFun.cpp" \
       -L"$HERE" -lfemh_oracle -Wl,-rpath,'$ORIGIN/..' -fopenmp
 fi
 echo "built $OUT"

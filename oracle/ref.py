@@ -59,15 +59,30 @@ def nc_coarsen(materials: np.ndarray, E, nu, densities, stype: int = CUBIC):
     return tv, pv[:k]
 
 
-def fastfem(n: int, x0: np.ndarray, nu: float, G0: np.ndarray, wG: np.ndarray, m0: float, mw: float):
-    """The reference's FEM3DFun on an n^3 cell with an m^3 PiecewiseConstant3D
-    field (x0 of m^3 parameters): dict of G (upper triangle, as the reference
-    fills it), f, df (m^3), distribution (n^3), density, status."""
+FIELD_PLAIN, FIELD_SYM, FIELD_CUBIC = 0, 1, 2
+
+
+def field_index(kind: int, m: int, x) -> int:
+    """The parameter the reference's field (kind: PiecewiseConstant3D /
+    Sym3D / Cubic3D, m^3 parameters) assigns to the point x."""
+    L = _load("libfastfem_ref.so")
+    if L is None:
+        return None
+    L.ref_field_index.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 3
+    L.ref_field_index.restype = ctypes.c_int
+    return int(L.ref_field_index(kind, m, *[float(v) for v in x]))
+
+
+def fastfem(n: int, x0: np.ndarray, nu: float, G0: np.ndarray, wG: np.ndarray, m0: float, mw: float,
+            kind: int = FIELD_PLAIN):
+    """The reference's FEM3DFun on an n^3 cell with an m^3 field of `kind`
+    (x0 of m^3 parameters): dict of G (upper triangle, as the reference fills
+    it), f, df (m^3), distribution (n^3), density, status."""
     L = _load("libfastfem_ref.so")
     if L is None:
         return None
     dp = ctypes.POINTER(ctypes.c_double)
-    L.ref_ff_eval.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp, ctypes.c_double,
+    L.ref_ff_eval.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp, ctypes.c_double,
                               ctypes.c_double, dp, dp, dp, dp, dp]
     L.ref_ff_eval.restype = ctypes.c_int
     x0 = np.ascontiguousarray(x0, dtype=np.float64).ravel()
@@ -77,7 +92,7 @@ def fastfem(n: int, x0: np.ndarray, nu: float, G0: np.ndarray, wG: np.ndarray, m
     wG = np.ascontiguousarray(wG, dtype=np.float64)
     G, f, df = np.zeros(36), np.zeros(1), np.zeros(m ** 3)
     dist, dens = np.zeros(n ** 3), np.zeros(1)
-    st = L.ref_ff_eval(n, m, nu, x0.ctypes.data_as(dp), G0.ctypes.data_as(dp), wG.ctypes.data_as(dp), m0, mw,
+    st = L.ref_ff_eval(n, m, kind, nu, x0.ctypes.data_as(dp), G0.ctypes.data_as(dp), wG.ctypes.data_as(dp), m0, mw,
                        G.ctypes.data_as(dp), f.ctypes.data_as(dp), df.ctypes.data_as(dp),
                        dist.ctypes.data_as(dp), dens.ctypes.data_as(dp))
     return {"G": G.reshape(6, 6), "f": float(f[0]), "df": df, "distribution": dist.reshape(n, n, n),

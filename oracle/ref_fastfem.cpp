@@ -6,7 +6,8 @@
 // is absent from the reference tree: oracle/ref_shim/ holds stand-in headers
 // whose Homogenize() runs the oracle's solve.  TEST INFRASTRUCTURE ONLY.
 //
-// ref_ff_eval: an n^3 cell, an m^3 PiecewiseConstant3D field with parameters x0, targets
+// ref_ff_eval: an n^3 cell, an m^3 field of `kind` (0 PiecewiseConstant3D,
+// 1 PiecewiseConstantSym3D, 2 PiecewiseConstantCubic3D) with parameters x0, targets
 // G0 / weights wG (6x6 row major), density target m0 and weight mw; set up as
 // fast_fem/run3d.cpp:117-164 (initFEM) and :166-202 (run3D) set up the
 // function -- lattice edge 1/n, Ke0 = the element stiffness of that edge
@@ -18,9 +19,44 @@
 
 #include "FEM3DFun.hpp"
 #include "PiecewiseConstant3D.hpp"
+#include "PiecewiseConstantCubic3D.hpp"
+#include "PiecewiseConstantSym3D.hpp"
 #include "femh_oracle.h"
 
-extern "C" int ref_ff_eval(int n, int m, double nu, const double* x0, const double* G0, const double* wG, double m0,
+namespace {
+// field kind 0: PiecewiseConstant3D, 1: PiecewiseConstantSym3D, 2: PiecewiseConstantCubic3D
+RealField* make_field(int kind, int m) {
+  if (kind == 1) {
+    PiecewiseConstantSym3D* f = new PiecewiseConstantSym3D();
+    f->allocate(m, m, m);
+    return f;
+  }
+  if (kind == 2) {
+    PiecewiseConstantCubic3D* f = new PiecewiseConstantCubic3D();
+    f->allocate(m, m, m);
+    return f;
+  }
+  PiecewiseConstant3D* f = new PiecewiseConstant3D();
+  f->allocate(m, m, m);
+  return f;
+}
+}  // namespace
+
+// Parameter index that the reference's field of this kind (m^3 parameters)
+// gives the point x (its df(x): one index, weight 1), or -1.
+extern "C" int ref_field_index(int kind, int m, double x, double y, double z) {
+  RealField* f = make_field(kind, m);
+  Eigen::VectorXd c(3);
+  c << x, y, z;
+  Eigen::SparseVector<double> d = f->df(c);
+  int idx = -1;
+  for (Eigen::SparseVector<double>::InnerIterator it(d); it; ++it)
+    if (it.value() == 1.0) idx = (int)it.index();
+  delete f;
+  return idx;
+}
+
+extern "C" int ref_ff_eval(int n, int m, int kind, double nu, const double* x0, const double* G0, const double* wG, double m0,
                            double mw, double* G_out, double* f_out, double* df_out, double* dist_out,
                            double* density_out) {
   const int nv = n * n * n;
@@ -40,12 +76,11 @@ extern "C" int ref_ff_eval(int n, int m, double nu, const double* x0, const doub
   Field<T, 3> coef;
   coef.Resize(Eigen::Vector3i(n, n, n));
   fun.fem.variable_coef = &coef;
-  PiecewiseConstant3D field;
-  field.allocate(m, m, m);
-  fun.field = &field;
+  RealField* field = make_field(kind, m);
+  fun.field = field;
   fun.gridSize[0] = fun.gridSize[1] = fun.gridSize[2] = n;
   fun.distribution.resize(nv);
-  fun.param = field.param;
+  fun.param = field->param;
   fun.initArrays();
   for (int i = 0; i < 6; ++i)
     for (int j = 0; j < 6; ++j) {
@@ -66,5 +101,6 @@ extern "C" int ref_ff_eval(int n, int m, double nu, const double* x0, const doub
   for (int i = 0; i < nv; ++i) dist_out[i] = fun.distribution[i];
   *density_out = fun.density;
   fun.hom = 0;
+  delete field;
   return hom.status;
 }

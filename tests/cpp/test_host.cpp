@@ -116,6 +116,16 @@ int main(int argc, char** argv) {
     print_vec("ff_G0", std::vector<double>(fb.G0.begin(), fb.G0.end()));
     print_vec("ff_wG", std::vector<double>(fb.wG.begin(), fb.wG.end()));
     print_vec("ff_df", gb);
+    // the same with run3D's cubic-symmetric field (fast_fem/run3d.cpp:176-182)
+    PiecewiseConstantCubic3D fc;
+    fc.allocate(4, 4, 4);
+    fb.field = &fc;
+    fb.setParam(x4);
+    const double fvc = fb.f();
+    std::vector<double> gc = fb.df();
+    std::printf("\"ffc_f\": %.17g,\n", fvc);
+    print_vec("ffc_G", std::vector<double>(fb.G.begin(), fb.G.end()));
+    print_vec("ffc_df", gc);
   }
   // ---------------------------------------------------------------- 2
   NumericalCoarseningUsingMultigrid nc;

@@ -166,6 +166,18 @@ int main() {
   std::printf("\"fun_density\": %.17g,\n", fun.density);
   std::printf("\"fun_f\": %.17g,\n", fun.f());
   print_vec("fun_df", fun.df());
+  {   // voxel -> parameter maps of the symmetric fields (3^3 parameters on a 7 x 8 x 9 grid)
+    const int n3[3] = {7, 8, 9};
+    PiecewiseConstantSym3D sym;
+    sym.allocate(3, 3, 3);
+    PiecewiseConstantCubic3D cub;
+    cub.allocate(3, 3, 3);
+    std::vector<int> ms, mc;
+    sym.voxelMap(n3, ms);
+    cub.voxelMap(n3, mc);
+    print_vec("map_sym", std::vector<double>(ms.begin(), ms.end()));
+    print_vec("map_cubic", std::vector<double>(mc.begin(), mc.end()));
+  }
   std::printf("\"ok\": true\n}\n");
   return 0;
 }

@@ -102,8 +102,9 @@ def test_fem3dfun_matches_reference_fast_fem(host_out):
     """femh_host::FEM3DFun (GPU solve, energy and adjoint) against the
     reference's own fast_fem FEM3DFun (fast_fem/FEM3DFun.cpp:128-268, built by
     oracle/build_ref.sh with the oracle's solve behind stand-in topoOptLib
-    headers) on an 8^3 cell over a 4^3 field: the upper triangle of G (the part
-    the reference fills) and f within the FP64 bar 1e-8, df within 1e-8."""
+    headers) on an 8^3 cell over a 4^3 field, a PiecewiseConstant3D one and
+    run3D's PiecewiseConstantCubic3D one: the upper triangle of G (the part the
+    reference fills) and f within the FP64 bar 1e-8, df within 1e-8."""
     from oracle import ref as R
     if not R.available("libfastfem_ref.so"):
         pytest.skip("oracle/_ref/libfastfem_ref.so not built")
@@ -117,6 +118,14 @@ def test_fem3dfun_matches_reference_fast_fem(host_out):
     assert host_out["ff_f"] == pytest.approx(r["f"], rel=1e-8)
     df = np.array(host_out["ff_df"])
     assert np.abs(df - r["df"]).max() < 1e-8 * np.abs(r["df"]).max()
+    # run3D's cubic-symmetric field: the chain rule on the device (femh_field_gradient)
+    rc = R.fastfem(8, np.array(host_out["ff_x0"]), 0.3, G0, wG, 0.4, 0.1, kind=R.FIELD_CUBIC)
+    assert rc["status"] == 0
+    Gc = np.array(host_out["ffc_G"]).reshape(6, 6)
+    assert np.abs(Gc[iu] - rc["G"][iu]).max() < 1e-8 * np.abs(rc["G"]).max()
+    assert host_out["ffc_f"] == pytest.approx(rc["f"], rel=1e-8)
+    dfc = np.array(host_out["ffc_df"])
+    assert np.abs(dfc - rc["df"]).max() < 1e-8 * np.abs(rc["df"]).max()
 
 
 def test_force_driven_coarsening_matches_reference_code(host_out):

@@ -150,3 +150,20 @@ def test_fem3dfun_objective_and_chain_rule(out):
     # over the 2x2x2 voxels of each field parameter
     g = np.trace(wG * (G - G0)) + 0.7 / 64 * (density - 0.4)
     assert np.allclose(out["fun_df"], 8 * g, rtol=1e-13, atol=0)
+
+
+def test_symmetric_field_maps_match_reference(out):
+    """femh_host::PiecewiseConstantSym3D / Cubic3D assign every voxel centre of
+    a 7x8x9 grid the same parameter as the reference's own field classes
+    (fast_fem/PiecewiseConstantSym3D.cpp, PiecewiseConstantCubic3D.cpp, built
+    by oracle/build_ref.sh); the maps feed femh_field_gradient."""
+    from oracle import ref as R
+    if not R.available("libfastfem_ref.so"):
+        pytest.skip("oracle/_ref/libfastfem_ref.so not built")
+    n = (7, 8, 9)
+    for key, kind in (("map_sym", R.FIELD_SYM), ("map_cubic", R.FIELD_CUBIC)):
+        got = np.array(out[key]).astype(int)
+        want = [R.field_index(kind, 3, ((i + .5) / n[0], (j + .5) / n[1], (k + .5) / n[2]))
+                for i in range(n[0]) for j in range(n[1]) for k in range(n[2])]
+        assert np.array_equal(got, want), key
+    assert len(set(np.array(out["map_cubic"]).astype(int))) < len(set(np.array(out["map_sym"]).astype(int)))

@@ -96,3 +96,29 @@ def test_fastfem_energy_and_gradient_loops_vs_oracle(oracle, n, m):
     dfd = oracle.grad(rho, chi, wG * (Gref - G0), mat=mat) + (mw / rho.size) * (rho.mean() - m0)
     g = dfd.reshape(m, rep, m, rep, m, rep).sum(axis=(1, 3, 5)).ravel()
     assert np.abs(r["df"] - g).max() < 1e-10 * np.abs(g).max()
+
+
+
+@pytest.mark.skipif(not R.available("libfastfem_ref.so"), reason="oracle/_ref/libfastfem_ref.so not built")
+@pytest.mark.parametrize("kind", [R.FIELD_SYM, R.FIELD_CUBIC])
+def test_fastfem_symmetric_fields_vs_oracle(oracle, kind):
+    """The same loops over the mirror- and cubic-symmetric fields of
+    fast_fem/PiecewiseConstant{Sym,Cubic}3D.cpp (the cubic one is run3D's,
+    fast_fem/run3d.cpp:176-182): the chain rule sums every voxel into the
+    parameter the field assigns it."""
+    n, m = 8, 4
+    x0, G0, wG = _ff_case(n, m, seed=30 + kind)
+    nu, m0, mw = 0.3, 0.4, 0.1
+    r = R.fastfem(n, x0, nu, G0, wG, m0, mw, kind=kind)
+    assert r["status"] == 0
+    idx = np.array([R.field_index(kind, m, ((i + .5) / n, (j + .5) / n, (k + .5) / n))
+                    for i in range(n) for j in range(n) for k in range(n)])
+    rho = np.clip(x0[idx], 1e-3, 1.0).reshape(n, n, n)
+    assert np.array_equal(r["distribution"], rho)
+    mat = oracle.material(interp=oracle.INTERP_RAMP3, E_s=1.0, nu=nu)
+    C, chi, _, _, st = oracle.homogenize(rho, mat=mat, tol=1e-12, max_iter=100000)
+    iu = np.triu_indices(6)
+    assert np.abs(r["G"][iu] - C[iu]).max() < 1e-11 * np.abs(C).max()
+    dfd = oracle.grad(rho, chi, wG * (r["G"] - G0), mat=mat) + (mw / rho.size) * (rho.mean() - m0)
+    g = np.bincount(idx, weights=dfd.ravel(), minlength=m ** 3)
+    assert np.abs(r["df"] - g).max() < 1e-10 * np.abs(g).max()
