@@ -6,6 +6,7 @@
 // SamplesGenerator/NumericalCoarseningUsingMultiGrid.cpp:221-345.  There is no
 // CPU fallback: every numeric step below is one of this library's kernels.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdint>
@@ -1707,6 +1708,7 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
   };
   capture();
   int done = 0;
+  const auto t_start = std::chrono::steady_clock::now();
   try {
     while (true) {
       if (exec) {
@@ -1730,6 +1732,10 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
         if (H->state[t].active) keep[t / kNumRhs] = 1;
       for (int ci = 0; ci < nc; ++ci) alive += keep[ci];
       if (alive == 0 || done > max_iter + chunk) break;
+      if (verbose())
+        std::fprintf(stderr, "[femh] pcg: %.3f s, %d iterations, %d of %d cells iterating\n",
+                     std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count(), done,
+                     alive, nc);
       if (nc > 1 && 2 * alive <= listed) {   // at least half of the listed cells finished: compact
         if (full.empty()) {
           full.resize(H->levels.size());
