@@ -115,13 +115,14 @@ def measured_peaks():
 
 
 def engine_source_sha() -> str:
-    """Hash of the engine's CUDA/C++ sources: ties a DRAM-traffic capture to
-    the code it measured."""
+    """Hash of the engine's device code (the kernel headers of fem_b200/csrc):
+    ties a DRAM-traffic capture to the kernels it measured."""
     import hashlib
     h = hashlib.sha256()
     base = os.path.join(ROOT, "fem_b200", "csrc")
     for f in sorted(os.listdir(base)):
-        h.update(open(os.path.join(base, f), "rb").read())
+        if f.endswith(".cuh"):
+            h.update(open(os.path.join(base, f), "rb").read())
     return h.hexdigest()[:16]
 
 
@@ -203,8 +204,9 @@ def batched_uneven(F, local: int, ncell: int, world: int = 1, rank: int = 0, fp6
     e.close()
     its = np.array([max(i["iterations"]) for i in infos])
     bad = int(max_over_ranks(sum(1 for i in infos if i["status"] != 0), device="cuda"))
+    solve_s = max((i["solve_ms"] for i in infos), default=0.0) / 1e3   # device time of the solve proper
     out = {"cells": len(cells), "voxels": int(sum(c.size for c in cells)), "ranks": world,
-           "cells_per_s": len(cells) / t_batch, "seconds": t_batch,
+           "cells_per_s": len(cells) / t_batch, "seconds": t_batch, "solve_seconds_rank0": solve_s,
            "calls_per_rank": int(max(1, np.ceil(sum(need) / (0.92 * avail)))),
            "device_bytes_needed_rank0": float(sum(need)),
            "iterations_p50_p90_max_rank0": [int(np.percentile(its, 50)), int(np.percentile(its, 90)), int(its.max())],
