@@ -1236,7 +1236,8 @@ void autotune_level0_fp64(femh_handle* H) {
   std::vector<int> vars64 = {1, 2};
   if (L.bulk_ok64) vars64.push_back(6);
   if (H->cfg.stencil_variant == 6 && L.bulk_ok64) vars64 = {6};
-  for (int var : vars64)
+  for (int var : vars64) {   // pruned as in autotune_levels
+    float var_best = 1e30f;
     for (int cand : cands) {
       build_stencil_units64(H, L, cand, var);
       float ms_min = 1e30f;
@@ -1249,6 +1250,7 @@ void autotune_level0_fp64(femh_handle* H) {
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, H->ev0, H->ev1));
         ms_min = std::min(ms_min, ms);
+        if (rep >= 1 && ms_min > 2.0f) break;
       }
       if (verbose()) std::fprintf(stderr, "[femh] tune level 0 fp64 variant %d chunk %d: %.4f ms\n", var, cand, ms_min);
       if (ms_min < best_ms) {
@@ -1256,7 +1258,10 @@ void autotune_level0_fp64(femh_handle* H) {
         best = cand;
         best_var = var;
       }
+      var_best = std::min(var_best, ms_min);
+      if (ms_min > 1.25f * var_best) break;
     }
+  }
   build_stencil_units64(H, L, best, best_var);
   H->tune_cache[key] = best * 16 + best_var;
 }
@@ -1302,7 +1307,11 @@ void autotune_levels(femh_handle* H, bool mg) {
     if (std::is_same<T, float>::value && L.bulk_ok) vars.push_back(5);
     if (std::is_same<T, double>::value && L.bulk_ok64) vars.push_back(6);
     if (H->cfg.stencil_variant > 0) vars = {H->cfg.stencil_variant};
-    for (int var : vars)
+    // chunks in increasing order: a variant's scan stops once a chunk is 25% slower
+    // than its best so far (the time is unimodal in the chunk); launches of a few
+    // milliseconds are stable after two samples
+    for (int var : vars) {
+    float var_best = 1e30f;
     for (int cand : cands) {
       L.variant = var;
       build_stencil_units(H, L, cand);
@@ -1316,6 +1325,7 @@ void autotune_levels(femh_handle* H, bool mg) {
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, H->ev0, H->ev1));
         ms_min = std::min(ms_min, ms);
+        if (rep >= 1 && ms_min > 2.0f) break;
       }
       if (verbose()) std::fprintf(stderr, "[femh] tune level %zu variant %d chunk %d: %.4f ms\n", l, var, cand, ms_min);
       if (ms_min < best_ms) {
@@ -1323,6 +1333,9 @@ void autotune_levels(femh_handle* H, bool mg) {
         best = cand;
         best_var = var;
       }
+      var_best = std::min(var_best, ms_min);
+      if (ms_min > 1.25f * var_best) break;
+    }
     }
     L.variant = best_var;
     build_stencil_units(H, L, best);

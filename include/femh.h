@@ -77,7 +77,10 @@ typedef struct {
   int max_iter;           /* CG iterations (plain) / inner iterations per outer step (mixed) */
   double inner_tol;       /* mixed: relative reduction asked of each inner solve */
   int max_outer;          /* mixed: defect-correction steps */
-  int store_bf16;         /* mixed: bf16 storage of search directions and rho */
+  int store_bf16;         /* mixed: bf16 storage of search directions and rho.  Converges on
+                             small cells (<= 32^3 tested); on the 128^3 smooth and 256^3
+                             binary benchmark cells CG then stalls near 1e-4 (the rounded
+                             search directions lose conjugacy): keep 0 there */
   int graph_chunk;        /* CG iterations per captured CUDA graph (0 = no graphs) */
   int coarse_avg;         /* coarse voxel modulus from its 8 children: 0 arithmetic mean
                              (rediscretisation of the mean), 1 geometric, 2 harmonic */
