@@ -37,7 +37,7 @@ def max_over_ranks(value: float, device=None) -> float:
 
 
 def batch_sharded(engine, cells: Sequence, dLdC=None, weights: Sequence[float] | None = None,
-                  allow_unconverged: bool = False):
+                  allow_unconverged: bool = False, gather_grads: bool = True):
     """Independent cells over the ranks of the default process group: each rank
     solves its share (`shard`, weighted by voxels unless `weights` is given) in
     its own batched engine calls, then the results are gathered in cell order
@@ -45,7 +45,10 @@ def batch_sharded(engine, cells: Sequence, dLdC=None, weights: Sequence[float] |
     The reference's sample generator fans cells out over 8 OpenMP threads
     (SamplesGenerator/SamplesGeneratorImpl.cpp:3707-3719); here one rank per
     GPU takes that role.  Returns (C [n,6,6], infos, dL/drho list or None)
-    like Engine.batch; every rank must call it with the same cells."""
+    like Engine.batch; every rank must call it with the same cells.  The
+    gradients are one value per voxel (1.4 GB for the 4096-cell set):
+    gather_grads=False keeps each rank's own (the other cells' entries are
+    None)."""
     import numpy as np
     import torch.distributed as dist
     on = dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1
@@ -59,12 +62,14 @@ def batch_sharded(engine, cells: Sequence, dLdC=None, weights: Sequence[float] |
                                        allow_unconverged=allow_unconverged)
     else:
         C, infos, grads = np.zeros((0, 6, 6)), [], ([] if dl is not None else None)
-    part = (mine, C, infos, grads)
+    part = (mine, C, infos, grads if gather_grads else None)
     parts = [None] * world
     if on:
         dist.all_gather_object(parts, part)
     else:
         parts = [part]
+    if not gather_grads and grads is not None:   # this rank's own gradients stay local
+        parts[rank] = (mine, C, infos, grads)
     Cs = np.zeros((len(cells), 6, 6))
     all_infos = [None] * len(cells)
     all_grads = [None] * len(cells) if dl is not None else None
@@ -72,6 +77,6 @@ def batch_sharded(engine, cells: Sequence, dLdC=None, weights: Sequence[float] |
         for k, i in enumerate(idx):
             Cs[i] = Cp[k]
             all_infos[i] = ip[k]
-            if all_grads is not None:
+            if all_grads is not None and gp is not None:
                 all_grads[i] = gp[k]
     return Cs, all_infos, all_grads
