@@ -291,6 +291,10 @@ struct UnitList {
   StencilUnit* d_su = nullptr;
   std::vector<NodeUnit> nu;
   NodeUnit* d_nu = nullptr;
+  // persistent staged kernel (variant 7): CTA b runs units [cta[b], cta[b+1])
+  std::vector<int> cta;
+  int* d_cta = nullptr;
+  int cta_cap = 0;   // entries allocated at d_cta
 };
 
 // Stencil units of one z extent: entries [b, e) of a unit list sorted by z extent.
@@ -409,6 +413,11 @@ struct femh_handle {
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int wait_limit = kWaitLimit;   // try_wait rounds of the staged kernels' stage waits
+  int nsm = 1;                   // multiprocessors of the device (persistent stencil CTAs)
+  // persistent stencil CTAs are split evenly over the six load cases; the inner
+  // solves of defect correction finish their load cases at different times
+  // (the CTAs of a finished one would idle), so they run one CTA per unit
+  bool persist_ok = true;
   int* d_loop = nullptr;         // CG iterations run on the device in the current solve (WHILE-node count)
   int* d_err = nullptr;   // [0] set by a stencil kernel whose bounded wait ran out,
                           // [1] by k_coef on a NaN, infinite or negative density
@@ -511,7 +520,7 @@ MatLaw make_law(const femh_config& c) {
 void add_stencil_units(std::vector<StencilUnit>& out, int cellidx, const CellDesc& cd, int NT,
                        int& slot, int chunk_req = 0, int variant = 2) {
   const int R = NT / cd.nz;
-  const bool two_rows = variant == 2 || variant == 4 || variant == 5;
+  const bool two_rows = variant == 2 || variant == 4 || variant == 5 || variant == 7;
   const int maxrows = std::max(1, std::min(two_rows ? 2 * R - 1 : R - 1, cd.ny));
   const int ntiles = (cd.ny + maxrows - 1) / maxrows;
   const int chunk = chunk_req > 0 ? std::min(chunk_req, cd.nx)
@@ -545,7 +554,7 @@ template <typename T> size_t esize() { return sizeof(T); }
 // needs up to ~160 registers a thread, so it runs 384-thread CTAs where its
 // tiles still hold at least two thread rows.
 int variant_nt(int level_nt, int maxnz, int variant) {
-  if ((variant == 4 || variant == 5) && level_nt > 384 && 384 >= 2 * maxnz) return 384;
+  if ((variant == 4 || variant == 5 || variant == 7) && level_nt > 384 && 384 >= 2 * maxnz) return 384;
   return level_nt;
 }
 
@@ -579,6 +588,35 @@ void group_units(const Level& L, std::vector<StencilUnit>& su, UnitGroups& g, bo
       g.e.back() = i + 1;
     }
   }
+}
+
+// Persistent staged kernel (variant 7): one CTA per multiprocessor, the six
+// load cases in blockIdx.y, so P = SMs / 6 CTAs per load case; CTA b runs the
+// consecutive units [cta[b], cta[b+1]) of the list, the cut points balancing
+// x planes (the kernel's steps).  The table lives at a fixed device address
+// (capacity P + 1), rewritten in place when the list changes (batch
+// compaction), so captured launches stay valid for the same P.
+void build_cta_table(femh_handle* H, const Level& L, UnitList& ul, bool upload_new) {
+  if (L.variant != 7 || L.grouped) {
+    ul.cta.clear();
+    return;
+  }
+  const int P = std::max(1, std::min(H->nsm / kNumRhs, (int)ul.su.size()));
+  long long tot = 0;
+  for (const auto& u : ul.su) tot += u.len;
+  ul.cta.assign(P + 1, (int)ul.su.size());
+  ul.cta[0] = 0;
+  long long acc = 0;
+  int p = 1;
+  for (int k = 0; k < (int)ul.su.size() && p < P; ++k) {
+    acc += ul.su[k].len;
+    while (p < P && acc * P >= tot * p) ul.cta[p++] = k + 1;
+  }
+  if (upload_new || ul.d_cta == nullptr || ul.cta_cap < P + 1) {
+    ul.cta_cap = std::max(P + 1, H->nsm / kNumRhs + 1);
+    ul.d_cta = H->setup.arr<int>(ul.cta_cap);
+  }
+  CK(cudaMemcpyAsync(ul.d_cta, ul.cta.data(), sizeof(int) * ul.cta.size(), cudaMemcpyHostToDevice, H->stream));
 }
 
 }  // namespace
@@ -671,7 +709,7 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   int variant = use64 ? L.variant64 : L.variant;
   if (!std::is_same<T, float>::value) {   // packed-FP32 kernels: FP64 twin with the same units
     if (variant == 3) variant = 1;
-    if (variant == 4 || variant == 5) variant = 2;
+    if (variant == 4 || variant == 5 || variant == 7) variant = 2;
   } else if (variant == 6) {   // the staged FP64 kernel's FP32 twin has the same units
     variant = 1;
   }
@@ -683,12 +721,19 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
     if (!(ok && L.bulk_ok64 && al(in) && al(out) && al(kc) && al(L.invd) && (!b || al(b)) && L.ntot % 4 == 0))
       variant = 1;
   }
+  bool persistent = false;
+  if (variant == 7) {   // the staged kernel as persistent CTAs over the list's CTA table
+    persistent = !use64 && !L.grouped && ul.cta.size() >= 2 && H->persist_ok;
+    variant = 5;
+  }
   if (variant == 5) {   // bulk-copy staging: FP32 storage, 16-byte aligned rows, eligible level
     const bool f32 = std::is_same<TIn, float>::value && std::is_same<TOut, float>::value &&
                      std::is_same<TB, float>::value && std::is_same<TC, float>::value;
     auto al = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
-    if (!(f32 && L.bulk_ok && al(in) && al(out) && al(kc) && al(L.invd) && (!b || al(b)) && L.ntot % 4 == 0))
+    if (!(f32 && L.bulk_ok && al(in) && al(out) && al(kc) && al(L.invd) && (!b || al(b)) && L.ntot % 4 == 0)) {
       variant = 4;
+      persistent = false;
+    }
   }
   StencilArgs<TIn, TOut, TB, TC> a;
   a.cells = L.d_cells;
@@ -705,12 +750,13 @@ void stencil(femh_handle* H, Level& L, bool smooth_only, const TIn* in, TOut* ou
   a.omega = omega;
   a.err = H->d_err;
   a.wait_limit = H->wait_limit;
+  a.cta_units = persistent ? ul.d_cta : nullptr;
   {
     const HadK& k = H->hk;
     const double kv[8] = {k.A, k.Bd - k.Bo, k.Bo, k.D1 - k.O1, k.O1, k.D2 - k.O2, k.O2, k.G};
     for (int i = 0; i < 8; ++i) a.kp[i] = make_float2((float)kv[i], (float)kv[i]);
   }
-  dim3 grid((unsigned)units.size(), kNumRhs);
+  dim3 grid((unsigned)(persistent ? ul.cta.size() - 1 : units.size()), kNumRhs);
   static const char* mode_names[] = {"apply", "apply_dot", "jacobi", "jacobi_dot", "resid"};
   char nm[64];
   snprintf(nm, sizeof nm, "stencil_%s_%s_L%d", sizeof(T) == 8 ? "f64" : "f32", mode_names[OUT], L.level);
@@ -1014,7 +1060,8 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
     L.bulk_ok = (L.nz_spec > 0 || L.grouped) && L.maxnz <= 128;
     L.bulk_ok64 = L.nz_spec > 0 || L.grouped;
     if (c.stencil_variant > 0) L.variant = c.stencil_variant;
-    if (L.variant == 5 && !L.bulk_ok) L.variant = 4;
+    if (L.variant == 7 && L.grouped) L.variant = 5;   // persistent CTAs need one z extent
+    if ((L.variant == 5 || L.variant == 7) && !L.bulk_ok) L.variant = 4;
     int ss = 0, sn = 0;
     for (int ci = 0; ci < (int)L.cells.size(); ++ci) {
       const CellDesc& cd = L.cells[ci];
@@ -1042,6 +1089,8 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
     L.all.d_nu = upload(ar, L.all.nu, s);
     L.smooth.d_su = upload(ar, L.smooth.su, s);
     L.smooth.d_nu = upload(ar, L.smooth.nu, s);
+    build_cta_table(H, L, L.all, true);
+    build_cta_table(H, L, L.smooth, true);
     L.d_su_sb = upload(ar, L.su_sb, s);
     L.d_su_se = upload(ar, L.su_se, s);
     L.d_nu_sb = upload(ar, L.nu_sb, s);
@@ -1150,6 +1199,8 @@ void set_units(femh_handle* H, Level& L, const FullLists& F, const std::vector<c
   };
   put_s(L.all.su, L.all.d_su, filt_s(F.all_su));
   put_s(L.smooth.su, L.smooth.d_su, filt_s(F.smooth_su));
+  build_cta_table(H, L, L.all, false);
+  build_cta_table(H, L, L.smooth, false);
   if (L.use64) put_s(L.su64, L.d_su64, filt_s(F.su64));
   group_units(L, L.all.su, L.gall, false);   // filtering keeps the z-extent order
   group_units(L, L.smooth.su, L.gsmooth, false);
@@ -1181,6 +1232,8 @@ void build_stencil_units(femh_handle* H, Level& L, int chunk) {
   L.smooth.d_su = upload(ar, L.smooth.su, s);
   L.d_su_sb = upload(ar, L.su_sb, s);
   L.d_su_se = upload(ar, L.su_se, s);
+  build_cta_table(H, L, L.all, true);
+  build_cta_table(H, L, L.smooth, true);
 }
 
 void build_stencil_units64(femh_handle* H, Level& L, int chunk, int variant) {
@@ -1305,6 +1358,9 @@ void autotune_levels(femh_handle* H, bool mg) {
     std::vector<int> vars = {1, 2};
     if (std::is_same<T, float>::value) vars = {2, 3, 4};
     if (std::is_same<T, float>::value && L.bulk_ok) vars.push_back(5);
+    // persistent CTAs (statically balanced) on single-cell levels: in a batch the
+    // cells converge at different iterations and one CTA per unit balances itself
+    if (std::is_same<T, float>::value && L.bulk_ok && !L.grouped && L.cells.size() == 1) vars.push_back(7);
     if (std::is_same<T, double>::value && L.bulk_ok64) vars.push_back(6);
     if (H->cfg.stencil_variant > 0) vars = {H->cfg.stencil_variant};
     // chunks in increasing order: a variant's scan stops once a chunk is 25% slower
@@ -1313,6 +1369,9 @@ void autotune_levels(femh_handle* H, bool mg) {
     for (int var : vars) {
     float var_best = 1e30f;
     for (int cand : cands) {
+      // persistent CTAs stream across units; their dot sums close per unit, so
+      // units shorter than 8 planes would add reductions without balancing better
+      if (var == 7 && cand < 8 && cand < maxnx) continue;
       L.variant = var;
       build_stencil_units(H, L, cand);
       float ms_min = 1e30f;
@@ -1896,6 +1955,11 @@ void solve_all(femh_handle* H, std::vector<femh_solve_info>& infos) {
       }
       if (!any) break;
       outer_done++;
+      H->persist_ok = false;
+      struct Restore {
+        femh_handle* h;
+        ~Restore() { h->persist_ok = true; }
+      } restore_{H};
       if (c.store_bf16)
         pcg<Prec<float, __nv_bfloat16, float, float, float>>(H, H->r64, kc32, c.max_iter, c.inner_tol, iters.data());
       else
@@ -2052,7 +2116,7 @@ void check_config(const femh_config& c) {
   if (!(c.tol > 0.0) || c.max_iter < 1) throw FemhError{FEMH_E_ARG, "tol > 0 and max_iter >= 1 are required"};
   if (c.precision == FEMH_MIXED && (!(c.inner_tol > 0.0) || c.max_outer < 1))
     throw FemhError{FEMH_E_ARG, "inner_tol > 0 and max_outer >= 1 are required"};
-  if (c.stencil_variant < 0 || c.stencil_variant > 6) throw FemhError{FEMH_E_ARG, "stencil_variant must be 0..6"};
+  if (c.stencil_variant < 0 || c.stencil_variant > 7) throw FemhError{FEMH_E_ARG, "stencil_variant must be 0..7"};
   if (!(c.cheb_ratio == 0.0 || c.cheb_ratio > 1.0)) throw FemhError{FEMH_E_ARG, "cheb_ratio must be 0 or > 1"};
   if (c.coarse_avg < 0 || c.coarse_avg > 2) throw FemhError{FEMH_E_ARG, "coarse_avg must be 0, 1 or 2"};
   if (!(c.E_s > 0.0) || c.E_min < 0.0 || !(c.rho_max >= c.rho_min))
@@ -2105,6 +2169,7 @@ femh_status femh_create(femh_handle** out, const femh_config* cfg) {
     H->cfg = *cfg;
     H->device = cfg->device;
     CK(cudaSetDevice(cfg->device));
+    CK(cudaDeviceGetAttribute(&H->nsm, cudaDevAttrMultiProcessorCount, cfg->device));
     CK(cudaStreamCreateWithFlags(&H->own_stream, cudaStreamNonBlocking));
     H->stream = H->own_stream;
     CK(cudaEventCreate(&H->ev0));

@@ -51,6 +51,7 @@ struct StencilArgs {
   float2 kp[8];          // FP32 pairs (x = y) of A, Bd-Bo, Bo, D1-O1, O1, D2-O2, O2, G
   int* err;              // set non-zero by a kernel whose bounded wait ran out
   int wait_limit;        // 0: every stage wait gives up at once (tests); else kWaitLimit rounds
+  const int* cta_units;  // staged FP32 kernel: CTA b runs units [cta_units[b], cta_units[b+1]); nullptr: unit b
 };
 
 template <typename T>
@@ -1265,6 +1266,14 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned
 // lanes of warp 0 issue against one mbarrier.  A ring of kBulkSlots stages
 // runs kBulkSlots-1 steps ahead of the one in use; no per-thread loads of
 // inputs remain.
+// Work of a CTA: one unit (a.cta_units == nullptr), or the run of units
+// [cta_units[b], cta_units[b+1]) as a persistent CTA.  Units that continue
+// each other along x (same cell and rows, adjacent x ranges) form one stream:
+// the carried planes pass from one unit to the next, so only a change of tile
+// pays the pipeline's fill (three stages) again.  The dot partial sums stay
+// per unit (written when a unit's last node plane is gathered), so results
+// are the same bits as one CTA per unit.  Stage g of a stream uses ring slot
+// (gbase + g) % kBulkSlots, gbase = stages of the CTA's earlier streams.
 // Requirements (checked by the host): nz % 4 == 0 on every cell, 16-byte
 // aligned arrays.  A tile has at most ny rows, so an array spans at most three
 // row segments: at most 20 copies per stage, one per lane of warp 0.
@@ -1275,30 +1284,23 @@ __global__ void __launch_bounds__(NT, 1)
 stencil2b_kernel(StencilArgs<float, float, float, float> a) {
   static_assert(NZ > 0 && NZ % 4 == 0, "staged rows need a compile-time z extent, multiple of 4");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const StencilUnit un = a.units[blockIdx.x];
   const int rhs = blockIdx.y;
-  const CellDesc cd = a.cells[un.cell];
-  if (a.stt && !a.stt[cd.id * kNumRhs + rhs].active) return;
-  const int nx = cd.nx, ny = cd.ny;
-  const int nz = NZ > 0 ? NZ : cd.nz;
-  const int TR = NT / nz;
+  int kb = blockIdx.x, ke = blockIdx.x + 1;   // units of this CTA: [kb, ke)
+  if (a.cta_units) {
+    kb = a.cta_units[blockIdx.x];
+    ke = a.cta_units[blockIdx.x + 1];
+  }
+  constexpr int nz = NZ;
+  constexpr int TR = NT / NZ;
   const int tid = threadIdx.x;
   const int t = tid / nz, z = tid - t * nz;
-  const int rows = un.rows;
-  const bool live = t < TR && 2 * t <= rows;
-  const bool own1 = live && 2 * t < rows;
-  const bool own2 = live && 2 * t + 1 < rows;
   const int zp = (z + 1 == nz) ? 0 : z + 1;
   const int zm = (z == 0) ? nz - 1 : z - 1;
-  auto wrapy = [&](int j) { j %= ny; return j < 0 ? j + ny : j; };
-  const int n1 = wrapy(un.j0 + 2 * t), n2 = wrapy(un.j0 + 2 * t + 1);
 
-  // stage layout (floats), sized for the largest tile so that every offset is
-  // a compile-time constant: U[3][NRU][nz], KC[NRK][nz], B[3][RB][nz], ID[RB][nz]
-  constexpr int TRc = NT / NZ, RB = 2 * TRc - 1, NRU = RB + 3, NRK = RB + 2;
+  constexpr int RB = 2 * TR - 1, NRU = RB + 3, NRK = RB + 2;
   constexpr int oK = 3 * NRU * NZ, oB = oK + NRK * NZ, oI = oB + 3 * RB * NZ;
-  constexpr int SS = (oI + RB * NZ + 3) & ~3;   // floats per stage, 16-byte multiple
-  const int PS = TR * 3 * nz;
+  constexpr int SS = (oI + RB * NZ + 3) & ~3;
+  constexpr int PS = TR * 3 * nz;
   float* stg = reinterpret_cast<float*>(smem_raw);
   f2* QAB = reinterpret_cast<f2*>(stg + kBulkSlots * SS);   // [2][TR][3][nz]
   f2* QCD = QAB + 2 * PS;
@@ -1307,260 +1309,294 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
   __shared__ int abort_flag;
   const int pt = t * 3 * nz;
   const int pa = (t + 1 < TR ? t + 1 : t) * 3 * nz;
-
   const long long st = a.ntot;
-  const int plane = ny * nz;
-  const int c1 = n1 * nz + z, c2 = n2 * nz + z;
-  float* obase = a.out + (long long)rhs * 3 * st + cd.off;
 
-  // copy descriptors: lane l of warp 0 owns copy l (at most 16 are used)
-  const char* src_base = nullptr;   // array base for this lane's copy (cell offset included)
-  int plane_lag = 0, src_off = 0, dst_off = 0, bytes = 0;
-  unsigned tx_total = 0;
-  if (tid < 32) {
-    int idx = 0;
-    auto seg = [&](const float* base, int lag, int row0, int nrows, int dst) {
-      int done = 0;
-      while (done < nrows) {
-        const int r0 = wrapy(row0 + done);
-        const int n = min(nrows - done, ny - r0);
-        if (idx == tid) {
-          src_base = reinterpret_cast<const char*>(base);
-          plane_lag = lag;
-          src_off = r0 * nz;
-          dst_off = dst + done * nz;
-          bytes = n * nz * 4;
-        }
-        tx_total += (unsigned)(n * nz * 4);
-        ++idx;
-        done += n;
-      }
-    };
-    for (int c = 0; c < 3; ++c) seg(a.u + ((long long)rhs * 3 + c) * st + cd.off, 1, un.j0 - 1, rows + 3, c * NRU * nz);
-    seg(a.kc + cd.off, 0, un.j0 - 1, rows + 2, oK);
-    if (OUT >= OUT_JACOBI) {
-      for (int c = 0; c < 3; ++c)
-        seg(a.b + ((long long)rhs * 3 + c) * st + cd.off, -1, un.j0, rows, oB + c * RB * nz);
-      if (OUT != OUT_RESID) seg(a.invd + cd.off, -1, un.j0, rows, oI);
-    }
-  }
-  // plane of this lane's next copy (stage 0 is plane i0-2+lag), advanced per issue
-  int pl_next = ((un.i0 - 2 + plane_lag) % nx + nx) % nx;
-  // stage g (= step g-1) is node plane i0-2+g of u, voxel plane i0-2+g of kc
-  // and node plane i0-3+g of b / invd; lag = plane offset relative to i0-2+g.
-  int issued = 0;   // stages issued so far (warp 0)
-  auto issue = [&](int g) {
-    issued = g + 1;
-    const int slot = g % kBulkSlots;
-    const unsigned bar = smem_addr(bars + slot);
-    if (tid == 0) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_expect_tx(bar, tx_total);
-    }
-    __syncwarp();
-    if (bytes > 0)
-      bulk_g2s(smem_addr(stg + slot * SS + dst_off), src_base + 4LL * ((long long)pl_next * plane + src_off),
-               (unsigned)bytes, bar);
-    if (++pl_next == nx) pl_next = 0;
-  };
-  const int G = un.len + 3;   // stages 0 .. len+2 (step -1 .. len+1)
   if (tid == 0) {
     for (int k = 0; k < kBulkSlots; ++k) mbar_init(smem_addr(bars + k), 1);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  if (tid < 32)
-    for (int g = 0; g < kBulkSlots && g < G; ++g) issue(g);
-  int waited = 0;   // stages 0 .. waited-1 completed for this thread (the exit drain starts there)
-  auto wait_stage = [&](int g) {
-    if (!mbar_wait_stage(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1), a.wait_limit == 0)) {
-      if (a.err) atomicExch(a.err, 1);
-      abort_flag = 1;
-    } else if (waited == g) {
-      waited = g + 1;   // a stage that timed out stays owed to the drain
-    }
-  };
 
-  f2 prv[3][4], car[3][4];
-  f2 own[3], u12[3], raw[3];
-  int pg = 0;
-  double acc = 0.0;
-#pragma unroll
-  for (int c = 0; c < 3; ++c) own[c] = u12[c] = raw[c] = p_bc(0.f);
+  unsigned gbase = 0;   // stages of the earlier streams (slot and phase of stage g: gbase + g)
+  for (int k = kb; k < ke;) {
+    const StencilUnit un = a.units[k];
+    const CellDesc cd = a.cells[un.cell];
+    int k2 = k + 1, len = un.len;
+    while (k2 < ke) {
+      const StencilUnit v = a.units[k2];
+      if (v.cell != un.cell || v.j0 != un.j0 || v.rows != un.rows || v.i0 != un.i0 + len) break;
+      len += v.len;
+      ++k2;
+    }
+    if (a.stt && !a.stt[cd.id * kNumRhs + rhs].active) {
+      k = k2;
+      continue;
+    }
+    const int nx = cd.nx, ny = cd.ny;
+    const int rows = un.rows;
+    const bool live = t < TR && 2 * t <= rows;
+    const bool own1 = live && 2 * t < rows;
+    const bool own2 = live && 2 * t + 1 < rows;
+    auto wrapy = [&](int j) { j %= ny; return j < 0 ? j + ny : j; };
+    const int n1 = wrapy(un.j0 + 2 * t), n2 = wrapy(un.j0 + 2 * t + 1);
+    const int plane = ny * nz;
+    const int c1 = n1 * nz + z, c2 = n2 * nz + z;
+    float* obase = a.out + (long long)rhs * 3 * st + cd.off;
 
-  auto patch = [&](const float* U, f2 (&h)[3][4], f2 (&mine)[3]) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float* Uc = U + c * NRU * nz;
-      const int r0 = (2 * t) * nz;
-      mine[c] = make_float2(Uc[r0 + nz + z], Uc[r0 + 2 * nz + z]);
-      const f2 up = make_float2(Uc[r0 + nz + zp], Uc[r0 + 2 * nz + zp]);
-      h[c][0] = make_float2(Uc[r0 + z], mine[c].x);
-      h[c][1] = make_float2(Uc[r0 + zp], up.x);
-      h[c][2] = mine[c];
-      h[c][3] = up;
-      had4_fwd(h[c]);
-    }
-  };
-  auto gather = [&](int buf, const float* S) {
-    const f2* Qab = QAB + buf * PS;
-    const f2* Qcd = QCD + buf * PS;
-    f2 y[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      y[c] = p_add(own[c], Qab[pt + c * nz + zm]);
-      y[c].y += Qcd[pa + c * nz + z].x + Qcd[pa + c * nz + zm].y;
-    }
-    float* ob = obase + pg;
-    const int r1 = (2 * t) * nz + z, r2 = r1 + nz;   // owned rows in the b / invd arrays
-    if (OUT == OUT_APPLY || OUT == OUT_APPLY_DOT) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if (own1) ob[c * st + c1] = y[c].x;
-        if (own2) ob[c * st + c2] = y[c].y;
-        if (OUT == OUT_APPLY_DOT) {
-          if (own1) acc += (double)u12[c].x * (double)y[c].x;
-          if (own2) acc += (double)u12[c].y * (double)y[c].y;
+    const char* src_base = nullptr;
+    int plane_lag = 0, src_off = 0, dst_off = 0, bytes = 0;
+    unsigned tx_total = 0;
+    if (tid < 32) {
+      int idx = 0;
+      auto seg = [&](const float* base, int lag, int row0, int nrows, int dst) {
+        int done = 0;
+        while (done < nrows) {
+          const int r0 = wrapy(row0 + done);
+          const int n = min(nrows - done, ny - r0);
+          if (idx == tid) {
+            src_base = reinterpret_cast<const char*>(base);
+            plane_lag = lag;
+            src_off = r0 * nz;
+            dst_off = dst + done * nz;
+            bytes = n * nz * 4;
+          }
+          tx_total += (unsigned)(n * nz * 4);
+          ++idx;
+          done += n;
         }
+      };
+      for (int c = 0; c < 3; ++c)
+        seg(a.u + ((long long)rhs * 3 + c) * st + cd.off, 1, un.j0 - 1, rows + 3, c * NRU * nz);
+      seg(a.kc + cd.off, 0, un.j0 - 1, rows + 2, oK);
+      if (OUT >= OUT_JACOBI) {
+        for (int c = 0; c < 3; ++c)
+          seg(a.b + ((long long)rhs * 3 + c) * st + cd.off, -1, un.j0, rows, oB + c * RB * nz);
+        if (OUT != OUT_RESID) seg(a.invd + cd.off, -1, un.j0, rows, oI);
       }
-    } else {
-      const bool pin1 = (pg + c1 == 0), pin2 = (pg + c2 == 0);
-      const float* Bs = S + oB;
-      f2 wd = p_bc(0.f);
-      if (OUT != OUT_RESID) {
-        const float* Is = S + oI;
-        wd = p_mul(p_bc((float)a.omega), make_float2(own1 ? Is[r1] : 0.f, own2 ? Is[r2] : 0.f));
+    }
+    int pl_next = ((un.i0 - 2 + plane_lag) % nx + nx) % nx;
+    int issued = 0;
+    auto issue = [&](int g) {
+      issued = g + 1;
+      const unsigned gg = gbase + (unsigned)g;
+      const int slot = (int)(gg % kBulkSlots);
+      const unsigned bar = smem_addr(bars + slot);
+      if (tid == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(bar, tx_total);
       }
+      __syncwarp();
+      if (bytes > 0)
+        bulk_g2s(smem_addr(stg + slot * SS + dst_off), src_base + 4LL * ((long long)pl_next * plane + src_off),
+                 (unsigned)bytes, bar);
+      if (++pl_next == nx) pl_next = 0;
+    };
+    const int G = len + 3;
+    if (tid < 32)
+      for (int g = 0; g < kBulkSlots && g < G; ++g) issue(g);
+    int waited = 0;
+    auto wait_stage = [&](int g) {
+      const unsigned gg = gbase + (unsigned)g;
+      if (!mbar_wait_stage(smem_addr(bars + gg % kBulkSlots), (gg / kBulkSlots) & 1u, a.wait_limit == 0)) {
+        if (a.err) atomicExch(a.err, 1);
+        abort_flag = 1;
+      } else if (waited == g) {
+        waited = g + 1;
+      }
+    };
+
+    f2 prv[3][4], car[3][4];
+    f2 own[3], u12[3], raw[3];
+    int pg = 0;
+    double acc = 0.0;
+    int ku = k, kend = un.len;   // unit of the gathered planes, and its end (plane index in the stream)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) own[c] = u12[c] = raw[c] = p_bc(0.f);
+
+    auto patch = [&](const float* U, f2 (&h)[3][4], f2 (&mine)[3]) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const f2 bv = make_float2(own1 ? Bs[c * RB * NZ + r1] : 0.f, own2 ? Bs[c * RB * NZ + r2] : 0.f);
-        const f2 d = p_sub(bv, y[c]);
-        if (OUT == OUT_RESID) {
-          if (own1) ob[c * st + c1] = pin1 ? 0.f : d.x;
-          if (own2) ob[c * st + c2] = pin2 ? 0.f : d.y;
-        } else {
-          const f2 xv = p_fma(wd, d, u12[c]);
-          if (own1) ob[c * st + c1] = xv.x;
-          if (own2) ob[c * st + c2] = xv.y;
-          if (OUT == OUT_JACOBI_DOT) {
-            if (own1) acc += (double)xv.x * (double)bv.x;
-            if (own2) acc += (double)xv.y * (double)bv.y;
+        const float* Uc = U + c * NRU * nz;
+        const int r0 = (2 * t) * nz;
+        mine[c] = make_float2(Uc[r0 + nz + z], Uc[r0 + 2 * nz + z]);
+        const f2 up = make_float2(Uc[r0 + nz + zp], Uc[r0 + 2 * nz + zp]);
+        h[c][0] = make_float2(Uc[r0 + z], mine[c].x);
+        h[c][1] = make_float2(Uc[r0 + zp], up.x);
+        h[c][2] = mine[c];
+        h[c][3] = up;
+        had4_fwd(h[c]);
+      }
+    };
+    auto gather = [&](int buf, const float* S) {
+      const f2* Qab = QAB + buf * PS;
+      const f2* Qcd = QCD + buf * PS;
+      f2 y[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        y[c] = p_add(own[c], Qab[pt + c * nz + zm]);
+        y[c].y += Qcd[pa + c * nz + z].x + Qcd[pa + c * nz + zm].y;
+      }
+      float* ob = obase + pg;
+      const int r1 = (2 * t) * nz + z, r2 = r1 + nz;
+      if (OUT == OUT_APPLY || OUT == OUT_APPLY_DOT) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (own1) ob[c * st + c1] = y[c].x;
+          if (own2) ob[c * st + c2] = y[c].y;
+          if (OUT == OUT_APPLY_DOT) {
+            if (own1) acc += (double)u12[c].x * (double)y[c].x;
+            if (own2) acc += (double)u12[c].y * (double)y[c].y;
+          }
+        }
+      } else {
+        const bool pin1 = (pg + c1 == 0), pin2 = (pg + c2 == 0);
+        const float* Bs = S + oB;
+        f2 wd = p_bc(0.f);
+        if (OUT != OUT_RESID) {
+          const float* Is = S + oI;
+          wd = p_mul(p_bc((float)a.omega), make_float2(own1 ? Is[r1] : 0.f, own2 ? Is[r2] : 0.f));
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const f2 bv = make_float2(own1 ? Bs[c * RB * NZ + r1] : 0.f, own2 ? Bs[c * RB * NZ + r2] : 0.f);
+          const f2 d = p_sub(bv, y[c]);
+          if (OUT == OUT_RESID) {
+            if (own1) ob[c * st + c1] = pin1 ? 0.f : d.x;
+            if (own2) ob[c * st + c2] = pin2 ? 0.f : d.y;
+          } else {
+            const f2 xv = p_fma(wd, d, u12[c]);
+            if (own1) ob[c * st + c1] = xv.x;
+            if (own2) ob[c * st + c2] = xv.y;
+            if (OUT == OUT_JACOBI_DOT) {
+              if (own1) acc += (double)xv.x * (double)bv.x;
+              if (own2) acc += (double)xv.y * (double)bv.y;
+            }
           }
         }
       }
-    }
-  };
+    };
 
-  // step -1 (stage 0): transformed patches of node plane i0-1
-  wait_stage(0);
-  if (live) {
-    f2 mine[3];
-    patch(stg, prv, mine);
+    wait_stage(0);
+    if (live) {
+      f2 mine[3];
+      patch(stg + (gbase % kBulkSlots) * SS, prv, mine);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      raw[c] = mine[c];
+      for (int c = 0; c < 3; ++c) {
+        raw[c] = mine[c];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) car[c][q] = p_bc(0.f);
+        for (int q = 0; q < 4; ++q) car[c][q] = p_bc(0.f);
+      }
     }
-  }
-  const int cellsz = nx * plane;
-  int pe_next = ((un.i0 - 1 + nx) % nx) * plane;   // voxel plane ie of step 0, advanced per step
-  for (int s = 0; s <= un.len + 1; ++s) {
-    const int g = s + 1;
-    wait_stage(g);
-    __syncthreads();   // stage g complete for all; Q[(s-1)&1] complete; slot of stage g-1 free
-    if (abort_flag) break;
-    if (tid < 32 && g + kBulkSlots - 1 < G) issue(g + kBulkSlots - 1);   // the slot of stage g-1
-    const float* S = stg + (g % kBulkSlots) * SS;
-    const int pe = pe_next;   // voxel plane ie
-    pe_next += plane;
-    if (pe_next >= cellsz) pe_next -= cellsz;
-    if (s >= 2 && live) gather((s - 1) & 1, S);
-    if (s > un.len || !live) continue;
-    f2 w[3][8];
-    f2 cur0[3];
-    {
-      f2 cur[3][4];
-      patch(S, cur, cur0);
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          if (q > 0) w[c][q] = p_add(cur[c][q], prv[c][q]);
-          w[c][4 + q] = p_sub(cur[c][q], prv[c][q]);
-          prv[c][q] = cur[c][q];
+    const int cellsz = nx * plane;
+    int pe_next = ((un.i0 - 1 + nx) % nx) * plane;
+    for (int s = 0; s <= len + 1; ++s) {
+      const int g = s + 1;
+      wait_stage(g);
+      __syncthreads();
+      if (abort_flag) break;
+      if (tid < 32 && g + kBulkSlots - 1 < G) issue(g + kBulkSlots - 1);
+      const float* S = stg + ((gbase + (unsigned)g) % kBulkSlots) * SS;
+      const int pe = pe_next;
+      pe_next += plane;
+      if (pe_next >= cellsz) pe_next -= cellsz;
+      if (s >= 2) {
+        if (live) gather((s - 1) & 1, S);
+        if (OUT == OUT_APPLY_DOT || OUT == OUT_JACOBI_DOT) {
+          if (s - 1 == kend) {   // gathered plane s-2 was the last one of unit ku
+            double v[1] = {acc};
+            block_reduce<1>(v, red);
+            if (tid == 0) a.partials[(long long)a.units[ku].slot * kNumRhs + rhs] = v[0];
+            acc = 0.0;
+            if (++ku < k2) kend += a.units[ku].len;
+          }
         }
-    }
-    {
-      const float* K = S + oK + (2 * t) * nz + z;
-      const f2 kv = make_float2(K[0], K[nz]);
-      const f2 A = p_mul(kv, a.kp[0]), Bdo = p_mul(kv, a.kp[1]), Bo = p_mul(kv, a.kp[2]);
-      const f2 D1o = p_mul(kv, a.kp[3]), O1 = p_mul(kv, a.kp[4]);
-      const f2 D2o = p_mul(kv, a.kp[5]), O2 = p_mul(kv, a.kp[6]), Gd = p_mul(kv, a.kp[7]);
-      {
-        const f2 m0 = w[0][4], m1 = w[1][2], m2 = w[2][1];
-        const f2 tt = p_mul(Bo, p_add(p_add(m0, m1), m2));
-        w[0][4] = p_fma(Bdo, m0, tt); w[1][2] = p_fma(Bdo, m1, tt); w[2][1] = p_fma(Bdo, m2, tt);
       }
+      if (s > len || !live) continue;
+      f2 w[3][8];
+      f2 cur0[3];
       {
-        const f2 sxz = p_mul(A, p_add(w[0][1], w[2][4]));
-        const f2 syz = p_mul(A, p_add(w[1][1], w[2][2]));
-        const f2 sxy = p_mul(A, p_add(w[0][2], w[1][4]));
-        w[0][1] = sxz; w[2][4] = sxz; w[1][1] = syz; w[2][2] = syz; w[0][2] = sxy; w[1][4] = sxy;
-      }
-      {
-        const f2 m0 = w[0][3], m1 = w[1][5], m2 = w[2][6];
-        const f2 tt = p_mul(O1, p_add(p_add(m0, m1), m2));
-        w[0][3] = p_fma(D1o, m0, tt); w[1][5] = p_fma(D1o, m1, tt); w[2][6] = p_fma(D1o, m2, tt);
-      }
-      {
-        const f2 x0 = w[1][3], x1 = w[0][5], tt = p_mul(O2, p_add(x0, x1));
-        w[1][3] = p_fma(D2o, x0, tt); w[0][5] = p_fma(D2o, x1, tt);
-      }
-      {
-        const f2 x0 = w[2][3], x1 = w[0][6], tt = p_mul(O2, p_add(x0, x1));
-        w[2][3] = p_fma(D2o, x0, tt); w[0][6] = p_fma(D2o, x1, tt);
-      }
-      {
-        const f2 x0 = w[2][5], x1 = w[1][6], tt = p_mul(O2, p_add(x0, x1));
-        w[2][5] = p_fma(D2o, x0, tt); w[1][6] = p_fma(D2o, x1, tt);
-      }
-      w[0][7] = p_mul(w[0][7], Gd); w[1][7] = p_mul(w[1][7], Gd); w[2][7] = p_mul(w[2][7], Gd);
-    }
-    f2* Qab = QAB + (s & 1) * PS;
-    f2* Qcd = QCD + (s & 1) * PS;
+        f2 cur[3][4];
+        patch(S, cur, cur0);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      f2 tot[4];
-      tot[0] = p_sub(car[c][0], w[c][4]);
-      car[c][0] = w[c][4];
+        for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int q = 1; q < 4; ++q) {
-        tot[q] = p_add(p_sub(w[c][q], w[c][4 + q]), car[c][q]);
-        car[c][q] = p_add(w[c][q], w[c][4 + q]);
+          for (int q = 0; q < 4; ++q) {
+            if (q > 0) w[c][q] = p_add(cur[c][q], prv[c][q]);
+            w[c][4 + q] = p_sub(cur[c][q], prv[c][q]);
+            prv[c][q] = cur[c][q];
+          }
       }
-      had4_inv(tot);
-      own[c] = make_float2(tot[0].y + tot[2].x, tot[2].y);
-      u12[c] = raw[c];
-      raw[c] = cur0[c];
-      if (s > 0) {
-        Qab[pt + c * nz + z] = make_float2(tot[1].y + tot[3].x, tot[3].y);
-        Qcd[pt + c * nz + z] = make_float2(tot[0].x, tot[1].x);
+      {
+        const float* K = S + oK + (2 * t) * nz + z;
+        const f2 kv = make_float2(K[0], K[nz]);
+        const f2 A = p_mul(kv, a.kp[0]), Bdo = p_mul(kv, a.kp[1]), Bo = p_mul(kv, a.kp[2]);
+        const f2 D1o = p_mul(kv, a.kp[3]), O1 = p_mul(kv, a.kp[4]);
+        const f2 D2o = p_mul(kv, a.kp[5]), O2 = p_mul(kv, a.kp[6]), Gd = p_mul(kv, a.kp[7]);
+        {
+          const f2 m0 = w[0][4], m1 = w[1][2], m2 = w[2][1];
+          const f2 tt = p_mul(Bo, p_add(p_add(m0, m1), m2));
+          w[0][4] = p_fma(Bdo, m0, tt); w[1][2] = p_fma(Bdo, m1, tt); w[2][1] = p_fma(Bdo, m2, tt);
+        }
+        {
+          const f2 sxz = p_mul(A, p_add(w[0][1], w[2][4]));
+          const f2 syz = p_mul(A, p_add(w[1][1], w[2][2]));
+          const f2 sxy = p_mul(A, p_add(w[0][2], w[1][4]));
+          w[0][1] = sxz; w[2][4] = sxz; w[1][1] = syz; w[2][2] = syz; w[0][2] = sxy; w[1][4] = sxy;
+        }
+        {
+          const f2 m0 = w[0][3], m1 = w[1][5], m2 = w[2][6];
+          const f2 tt = p_mul(O1, p_add(p_add(m0, m1), m2));
+          w[0][3] = p_fma(D1o, m0, tt); w[1][5] = p_fma(D1o, m1, tt); w[2][6] = p_fma(D1o, m2, tt);
+        }
+        {
+          const f2 x0 = w[1][3], x1 = w[0][5], tt = p_mul(O2, p_add(x0, x1));
+          w[1][3] = p_fma(D2o, x0, tt); w[0][5] = p_fma(D2o, x1, tt);
+        }
+        {
+          const f2 x0 = w[2][3], x1 = w[0][6], tt = p_mul(O2, p_add(x0, x1));
+          w[2][3] = p_fma(D2o, x0, tt); w[0][6] = p_fma(D2o, x1, tt);
+        }
+        {
+          const f2 x0 = w[2][5], x1 = w[1][6], tt = p_mul(O2, p_add(x0, x1));
+          w[2][5] = p_fma(D2o, x0, tt); w[1][6] = p_fma(D2o, x1, tt);
+        }
+        w[0][7] = p_mul(w[0][7], Gd); w[1][7] = p_mul(w[1][7], Gd); w[2][7] = p_mul(w[2][7], Gd);
       }
+      f2* Qab = QAB + (s & 1) * PS;
+      f2* Qcd = QCD + (s & 1) * PS;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        f2 tot[4];
+        tot[0] = p_sub(car[c][0], w[c][4]);
+        car[c][0] = w[c][4];
+#pragma unroll
+        for (int q = 1; q < 4; ++q) {
+          tot[q] = p_add(p_sub(w[c][q], w[c][4 + q]), car[c][q]);
+          car[c][q] = p_add(w[c][q], w[c][4 + q]);
+        }
+        had4_inv(tot);
+        own[c] = make_float2(tot[0].y + tot[2].x, tot[2].y);
+        u12[c] = raw[c];
+        raw[c] = cur0[c];
+        if (s > 0) {
+          Qab[pt + c * nz + z] = make_float2(tot[1].y + tot[3].x, tot[3].y);
+          Qcd[pt + c * nz + z] = make_float2(tot[0].x, tot[1].x);
+        }
+      }
+      pg = pe;
     }
-    pg = pe;
-  }
-  // drain: every issued stage completes before the CTA's shared memory goes
-  // (bounded; only reached with stages outstanding after an abort)
-  if (tid == 0) {
-    for (int g = waited; g < issued; ++g)
-      if (!mbar_wait(smem_addr(bars + g % kBulkSlots), (unsigned)((g / kBulkSlots) & 1))) break;
-  }
-  if (OUT == OUT_APPLY_DOT || OUT == OUT_JACOBI_DOT) {
-    double v[1] = {acc};
-    block_reduce<1>(v, red);
-    if (tid == 0) a.partials[(long long)un.slot * kNumRhs + rhs] = v[0];
+    if (abort_flag) {   // drain this stream's outstanding stages (bounded) and stop
+      if (tid == 0)
+        for (int g = waited; g < issued; ++g) {
+          const unsigned gg = gbase + (unsigned)g;
+          if (!mbar_wait(smem_addr(bars + gg % kBulkSlots), (gg / kBulkSlots) & 1u)) break;
+        }
+      break;
+    }
+    gbase += (unsigned)G;
+    k = k2;
+    __syncthreads();   // every read of this stream's stages and Q buffers is done before the next issues
   }
 }
 

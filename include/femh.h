@@ -91,9 +91,12 @@ typedef struct {
                              lanes, 5 as 4 with the inputs staged in shared memory by bulk
                              copies (3-5: FP32 operators; FP64 ones use 1 or 2), 6 one row
                              per thread in FP64 with staged inputs (FP64 operators; FP32
-                             ones use 1).  5 and 6 need every cell of a level to have a z
-                             extent in {16,24,32,48,64,128 (,256 for 6)} (levels of mixed
-                             extents launch one kernel per extent); elsewhere 4 and 1 run */
+                             ones use 1), 7 as 5 with one persistent CTA per multiprocessor
+                             running a balanced run of units (FP32 operators; levels of one
+                             z extent).  5-7 need every cell of a level to have a z extent
+                             in {16,24,32,48,64,128 (,256 for 6)} (levels of mixed extents
+                             launch one kernel per extent; 7 runs as 5 there); elsewhere 4
+                             and 1 run */
   int warm_start;         /* 1: a solve on the same cells as the handle's previous solve
                              starts from that solution (chi) instead of zero -- the
                              line-search / descent case of fast_fem/run3d.cpp:238-289;

@@ -54,7 +54,7 @@ def test_config_default_matches_binding(lib):
 def test_bad_config_rejected_before_device_use(lib):
     from fem_b200.femh import _Config
     lib.femh_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(_Config)]
-    for field, value in (("nu", 0.7), ("cheb_ratio", 0.5), ("cheb_ratio", -2.0), ("stencil_variant", 7)):
+    for field, value in (("nu", 0.7), ("cheb_ratio", 0.5), ("cheb_ratio", -2.0), ("stencil_variant", 8)):
         c = _Config()
         lib.femh_config_default(ctypes.byref(c))
         setattr(c, field, value)

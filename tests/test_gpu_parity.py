@@ -42,14 +42,14 @@ def test_apply_matches_oracle(femh, oracle, rng, shape):
     assert _rel(y, yo) < TOL_APPLY
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 7])
 @pytest.mark.parametrize("shape", [(16, 16, 16), (12, 8, 20), (8, 24, 24), (6, 10, 4), (8, 16, 128),
                                    (6, 20, 64), (4, 32, 32), (5, 11, 128), (3, 5, 16), (4, 6, 256)])
 def test_fp32_stencil_variants_match_oracle(femh, oracle, rng, shape, variant):
     """The FP32 kernels of the multigrid sweeps, each forced in turn: one voxel
     row per thread, two rows per thread, two load cases per thread in packed
-    FP32x2 lanes, two rows per thread in packed FP32x2 lanes, and the same with
-    its inputs staged by bulk copies.  z extents in the compile-time set run
+    FP32x2 lanes, two rows per thread in packed FP32x2 lanes, the same with
+    its inputs staged by bulk copies, and that one as persistent CTAs.  z extents in the compile-time set run
     the compile-time kernels (the staged one up to 128; at 256 it falls back
     to the unstaged packed kernel), the others (20, 4) the runtime-z kernels;
     in (3, 5, 16) and (16, 16, 16) one tile covers the whole y ring, so the

@@ -49,7 +49,7 @@ def test_operator_properties_128(femh, cell128):
     assert np.abs(Kt).max() <= 1e-12 * np.abs(Ku).max()
 
 
-@pytest.mark.parametrize("variant", [3, 4, 5])
+@pytest.mark.parametrize("variant", [3, 4, 5, 7])
 def test_fp32_packed_kernels_128(femh, cell128, variant):
     rng = np.random.default_rng(4)
     u = rng.standard_normal((6,) + cell128.shape + (3,))
@@ -78,3 +78,37 @@ def test_axis_swap_and_translation_64(femh):
     assert _rel(Cs, C[np.ix_(perm, perm)]) < TOL_FP64
     Ct, _ = e.homogenize(np.ascontiguousarray(np.roll(rho, (5, 7, 11), axis=(0, 1, 2))))
     assert _rel(Ct, C) < TOL_FP64
+
+
+def test_persistent_staged_kernel_same_bits_128(femh, cell128):
+    """The staged FP32 kernel as persistent CTAs (variant 7: one CTA per
+    multiprocessor and load case group, each streaming a balanced run of
+    units) against one CTA per unit (variant 5) on the same units: the
+    operator, and a whole mixed-precision solve whose V-cycles run the Jacobi,
+    residual and Jacobi+dot sweeps, give the same bits."""
+    rng = np.random.default_rng(6)
+    u = rng.standard_normal((6,) + cell128.shape + (3,))
+    e5 = femh.Engine(precision=femh.MIXED_PC, stencil_variant=5, autotune=0)
+    e7 = femh.Engine(precision=femh.MIXED_PC, stencil_variant=7, autotune=0)
+    assert np.array_equal(e5.apply_operator(cell128, u), e7.apply_operator(cell128, u))
+    C5, i5 = e5.homogenize(cell128)
+    C7, i7 = e7.homogenize(cell128)
+    assert i5["status"] == 0 and i7["status"] == 0
+    assert i5["iterations"] == i7["iterations"]
+    assert np.array_equal(C5, C7)
+
+
+def test_persistent_staged_kernel_batch(femh):
+    """Persistent CTAs whose runs span several cells of a batch, with the unit
+    lists compacted (and the CTA tables rebuilt) as cells converge: C^H and
+    iterations of every cell are the same bits as with one CTA per unit."""
+    from fem_b200 import fields
+    rhos = [fields.binary_cell(32, vf, seed=s) for s, vf in ((1, 0.25), (2, 0.5), (3, 0.35), (4, 0.6), (5, 0.45))]
+    rhos.append(fields.smooth_cell(32, 3.0, seed=9))
+    out = {}
+    for var in (5, 7):
+        C, infos, _ = femh.Engine(precision=femh.MIXED_PC, stencil_variant=var, autotune=0).batch(rhos, h=None)
+        out[var] = (C, [i["iterations"] for i in infos], [i["status"] for i in infos])
+    assert out[5][2] == [0] * len(rhos) and out[7][2] == [0] * len(rhos)
+    assert out[5][1] == out[7][1]
+    assert np.array_equal(out[5][0], out[7][0])
