@@ -141,8 +141,8 @@ def kernel_traffic(kernel: str):
 
 
 # ----------------------------------------------------------- CPU baseline --
-SOLVER = ("GMG-PCG: Jacobi 3+3 sweeps with Chebyshev-root weights, rediscretised coarse levels "
-          "down to <= 64 nodes, FP64 dense coarse solve")
+SOLVER = ("GMG-PCG: node-block (3x3) Jacobi 3+3 sweeps with Chebyshev-root weights, rediscretised coarse "
+          "levels down to <= 64 nodes, FP64 dense coarse solve")
 
 
 def workload_config(n: int, world: int) -> dict:
@@ -161,7 +161,7 @@ def cpu_baseline(rho, Ct):
     from oracle import oracle as O
     n = rho.shape[0]
     t0 = time.perf_counter()
-    C, chi, it, rel, st = O.mg_homogenize(rho, tol=1e-10)
+    C, chi, it, rel, st = O.mg_homogenize(rho, tol=1e-10, block=True)
     t1 = time.perf_counter()
     O.grad(rho, chi, 2 * (C - Ct))
     t2 = time.perf_counter()
@@ -192,8 +192,23 @@ def batched_uneven(F, local: int, ncell: int, world: int = 1, rank: int = 0, fp6
     mine = shard([float(c.size) for c in cells], world)[rank]
     my_cells = [cells[i] for i in mine]
     W = np.tile(np.diag([1.0, 1.0, 1.0, 0.5, 0.5, 0.5]), (len(my_cells), 1, 1))
+    # node-block smoothing (the default) where the set fits one call with it;
+    # otherwise point smoothing, which needs 24 B per node per level less
+    smoother, bj = "node-block Jacobi", 1
     e = F.Engine(F.Config(device=local, precision=F.MIXED_PC))
     need, avail = e.batch_memory([c.shape for c in my_cells])
+    if sum(need) > 0.92 * avail:
+        e.close()
+        e = F.Engine(F.Config(device=local, precision=F.MIXED_PC, block_jacobi=0))
+        need_b = sum(need)
+        need, avail = e.batch_memory([c.shape for c in my_cells])
+        if sum(need) <= 0.92 * avail:
+            bj = 0
+            smoother = f"point Jacobi (node-block needs {need_b / 1e9:.1f} GB, over one call's {0.92 * avail / 1e9:.1f} GB)"
+        else:
+            e.close()
+            e = F.Engine(F.Config(device=local, precision=F.MIXED_PC))
+            need, avail = e.batch_memory([c.shape for c in my_cells])
     e.batch(my_cells[:8], dLdC=W[:8], allow_unconverged=True)   # warm-up: library, autotuner code paths
     if world > 1:
         import torch.distributed as dist
@@ -212,9 +227,10 @@ def batched_uneven(F, local: int, ncell: int, world: int = 1, rank: int = 0, fp6
            "iterations_p50_p90_max_rank0": [int(np.percentile(its, 50)), int(np.percentile(its, 90)), int(its.max())],
            "not_converged_max_over_ranks": bad,
            "precision": "FP64 CG + FP32 multigrid, gradients contracted with a fixed dL/dC",
+           "smoother": smoother,
            "set": "fields.uneven_batch(4096, seed=7)"}
     if rank == 0:
-        e64 = F.Engine(F.Config(device=local, precision=F.FP64))
+        e64 = F.Engine(F.Config(device=local, precision=F.FP64, block_jacobi=bj))
         k = min(fp64_sample, len(cells))
         e64.homogenize(cells[0])
         t0 = time.perf_counter()
@@ -420,7 +436,7 @@ def run_reference(args, world, rank):
     Ct = target_tensor(n)
     warm = min(args.warmup, 3)
     for _ in range(warm):   # page the library and the OpenMP pool in on a small cell
-        O.mg_homogenize(fields.smooth_cell(32, 4.0, seed=2), tol=1e-10, want_chi=False)
+        O.mg_homogenize(fields.smooth_cell(32, 4.0, seed=2), tol=1e-10, want_chi=False, block=True)
     secs, cb = [], None
     t_start = time.perf_counter()
     while len(secs) < max(1, args.steps):

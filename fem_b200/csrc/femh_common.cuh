@@ -87,6 +87,27 @@ __device__ __forceinline__ void st_val(double* p, double v) { *p = v; }
 __device__ __forceinline__ void st_val(float* p, float v) { *p = v; }
 __device__ __forceinline__ void st_val(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
 
+// Damped-Jacobi direction at one node: d <- D^-1 d, D the point diagonal
+// (inverse id, the same for the 3 components) or, with binv != nullptr, the
+// node's 3x3 diagonal block of K (node-block Jacobi; the symmetric inverse
+// [xx, yy, zz, xy, xz, yz] stored at binv + 6 g, 8-byte aligned).
+template <typename T>
+__device__ __forceinline__ void jacobi_dir(const float* __restrict__ binv, long long g, T id, T (&d)[3]) {
+  if (binv) {
+    const float2 b01 = *reinterpret_cast<const float2*>(binv + 6 * g);
+    const float2 b23 = *reinterpret_cast<const float2*>(binv + 6 * g + 2);
+    const float2 b45 = *reinterpret_cast<const float2*>(binv + 6 * g + 4);
+    const T xx = (T)b01.x, yy = (T)b01.y, zz = (T)b23.x, xy = (T)b23.y, xz = (T)b45.x, yz = (T)b45.y;
+    const T d0 = d[0], d1 = d[1], d2 = d[2];
+    d[0] = xx * d0 + xy * d1 + xz * d2;
+    d[1] = xy * d0 + yy * d1 + yz * d2;
+    d[2] = xz * d0 + yz * d1 + zz * d2;
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) d[c] *= id;
+  }
+}
+
 // Warp + block reduction of nv doubles; result valid in thread 0.
 template <int NV>
 __device__ __forceinline__ void block_reduce(double (&v)[NV], double* smem /* >= 32*NV */) {

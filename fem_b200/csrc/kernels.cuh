@@ -128,6 +128,49 @@ __global__ void k_invdiag(const CellDesc* cells, const NodeUnit* units, const TC
   }
 }
 
+// Node-block Jacobi: D_n = the 3x3 diagonal block of K at node n = sum over
+// the 8 voxels at n of kc_e K0(1)_aa, a = the node's corner in voxel e.  The
+// cube's corner blocks are d I + o S_a, S_a(c1, c2) = sigma_c1 sigma_c2 off the
+// diagonal, sigma_c = 1 - 2 bit_c(a) (d = K0 diagonal, o = K0[0][1]), so
+// D_n = d (sum kc) I + o T_n with T_n(c1, c2) = sum_e kc_e sigma_c1 sigma_c2.
+// binv[6 (cd.off + n) + k] = the symmetric inverse, k = xx, yy, zz, xy, xz, yz
+// (FP32; 0 at the pinned node 0).
+template <typename TC>
+__global__ void k_invblock(const CellDesc* cells, const NodeUnit* units, const TC* kc, double d, double o,
+                           float* binv) {
+  const NodeUnit u = units[blockIdx.x];
+  const CellDesc cd = cells[u.cell];
+  #pragma unroll 4
+  for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
+    int i, j, k;
+    node_ijk(n, cd.ny, cd.nz, i, j, k);
+    double sum = 0.0, txy = 0.0, txz = 0.0, tyz = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int ax = (a >> 2) & 1, ay = (a >> 1) & 1, az = a & 1;
+      const double ke = (double)kc[cd.off + lin(wrap(i - ax, cd.nx), wrap(j - ay, cd.ny), wrap(k - az, cd.nz), cd.ny,
+                                                cd.nz)];
+      const double sx = 1.0 - 2.0 * ax, sy = 1.0 - 2.0 * ay, sz = 1.0 - 2.0 * az;
+      sum += ke;
+      txy += ke * sx * sy;
+      txz += ke * sx * sz;
+      tyz += ke * sy * sz;
+    }
+    const double A = d * sum, X = o * txy, Y = o * txz, Z = o * tyz;   // [[A X Y] [X A Z] [Y Z A]]
+    const double c00 = A * A - Z * Z, c11 = A * A - Y * Y, c22 = A * A - X * X;
+    const double c01 = Y * Z - X * A, c02 = X * Z - Y * A, c12 = X * Y - A * Z;
+    const double det = A * c00 + X * c01 + Y * c02;
+    const double r = (n == 0) ? 0.0 : 1.0 / det;
+    float* out = binv + 6 * (cd.off + n);
+    out[0] = (float)(c00 * r);
+    out[1] = (float)(c11 * r);
+    out[2] = (float)(c22 * r);
+    out[3] = (float)(c01 * r);
+    out[4] = (float)(c02 * r);
+    out[5] = (float)(c12 * r);
+  }
+}
+
 // Strain-driven load b^I_n = -sum_{e at n} c_e (K0(h) ue0^I(h))[a_n(e)]
 //   = -h * sum_e kc_e g1^I[a_n(e)]  (K0(h) = h K0(1), ue0(h) = h ue0(1), kc = c h).
 // Pinned node 0 gets 0.  One CTA per (unit, load case).
@@ -204,7 +247,7 @@ template <typename TV, typename TP, typename TQ, typename TZ>
 __global__ void k_cg_update(const CellDesc* cells, const NodeUnit* units, TV* __restrict__ x, TV* __restrict__ r, const TP* __restrict__ p,
                             const TQ* __restrict__ q, const float* __restrict__ invd, TZ* __restrict__ z0,
                             TZ* __restrict__ rm, double omega, const CGState* stt,
-                            double* __restrict__ part, long long ntot) {
+                            double* __restrict__ part, long long ntot, const float* __restrict__ binv) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cd = cells[u.cell];
@@ -216,6 +259,7 @@ __global__ void k_cg_update(const CellDesc* cells, const NodeUnit* units, TV* __
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
       const long long g = cd.off + n;
       const double id = (double)invd[g];
+      double rvs[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const long long o = ((long long)rhs * 3 + c) * ntot + g;
@@ -226,8 +270,14 @@ __global__ void k_cg_update(const CellDesc* cells, const NodeUnit* units, TV* __
         st_val(r + o, rv);
         v[0] += rv * rv;
         v[1] += rv * id * rv;
-        if (z0) st_val(z0 + o, omega * id * rv);
+        if (z0 && !binv) st_val(z0 + o, omega * id * rv);
         if (rm) st_val(rm + o, rv);
+        rvs[c] = rv;
+      }
+      if (z0 && binv) {   // node-block Jacobi: z0 = omega B r
+        jacobi_dir<double>(binv, g, 0.0, rvs);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) st_val(z0 + ((long long)rhs * 3 + c) * ntot + g, omega * rvs[c]);
       }
     }
   }
@@ -399,7 +449,7 @@ template <typename TF, typename TCo>
 __global__ void k_restrict(const CellDesc* fine, const CellDesc* coarse, const NodeUnit* units,
                            const TF* __restrict__ rf, TCo* __restrict__ bc, TCo* __restrict__ xc,
                            const float* __restrict__ invdc, double omega, const CGState* stt, long long ntf,
-                           long long ntc) {
+                           long long ntc, const float* __restrict__ binvc) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cc = coarse[u.cell], cf = fine[cc.parent];
@@ -432,10 +482,18 @@ __global__ void k_restrict(const CellDesc* fine, const CellDesc* coarse, const N
 #pragma unroll
     for (int c = 0; c < 3; ++c) st_val(bc + ((long long)rhs * 3 + c) * ntc + g, acc[c]);
     if (smooth) {
-      const double id = (double)invdc[g];
+      double bs[3];
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        st_val(xc + ((long long)rhs * 3 + c) * ntc + g, omega * id * (double)static_cast<TCo>(acc[c]));
+      for (int c = 0; c < 3; ++c) bs[c] = (double)static_cast<TCo>(acc[c]);   // b as stored
+      if (binvc) {
+        jacobi_dir<double>(binvc, g, 0.0, bs);
+      } else {
+        const double id = (double)invdc[g];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) bs[c] *= id;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) st_val(xc + ((long long)rhs * 3 + c) * ntc + g, omega * bs[c]);
     }
   }
 }
@@ -497,7 +555,7 @@ __global__ void k_prolong_add(const CellDesc* __restrict__ fine, const CellDesc*
 template <typename TB, typename TX>
 __global__ void k_jacobi0(const CellDesc* cells, const NodeUnit* units, const TB* __restrict__ b, TX* __restrict__ x,
                           TX* __restrict__ bcopy, const float* __restrict__ invd, double omega, const CGState* stt,
-                          long long ntot) {
+                          long long ntot, const float* __restrict__ binv) {
   const NodeUnit u = units[blockIdx.x];
   const int rhs = blockIdx.y;
   const CellDesc cd = cells[u.cell];
@@ -505,14 +563,22 @@ __global__ void k_jacobi0(const CellDesc* cells, const NodeUnit* units, const TB
   #pragma unroll 4
   for (long long n = u.begin + threadIdx.x; n < u.end; n += blockDim.x) {
     const long long g = cd.off + n;
-    const double id = (double)invd[g];
+    double bv[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long o = ((long long)rhs * 3 + c) * ntot + g;
-      const double bv = (double)ld_val(b + o);
-      st_val(x + o, omega * id * bv);
-      if (bcopy) st_val(bcopy + o, bv);
+      bv[c] = (double)ld_val(b + o);
+      if (bcopy) st_val(bcopy + o, bv[c]);
     }
+    if (binv) {
+      jacobi_dir<double>(binv, g, 0.0, bv);
+    } else {
+      const double id = (double)invd[g];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) bv[c] *= id;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) st_val(x + ((long long)rhs * 3 + c) * ntot + g, omega * bv[c]);
   }
 }
 

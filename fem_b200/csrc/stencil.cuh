@@ -29,7 +29,7 @@ namespace femh {
 enum OutMode : int {
   OUT_APPLY = 0,       // out = K u
   OUT_APPLY_DOT = 1,   // out = K u, partial u . K u
-  OUT_JACOBI = 2,      // out = u + omega * invd * (b - K u)
+  OUT_JACOBI = 2,      // out = u + omega * D^-1 (b - K u), D point or node-block diagonal
   OUT_JACOBI_DOT = 3,  // same, partial out . b
   OUT_RESID = 4,       // out = b - K u (pinned node 0 of each cell set to 0)
 };
@@ -52,6 +52,8 @@ struct StencilArgs {
   int* err;              // set non-zero by a kernel whose bounded wait ran out
   int wait_limit;        // 0: every stage wait gives up at once (tests); else kWaitLimit rounds
   const int* cta_units;  // staged FP32 kernel: CTA b runs units [cta_units[b], cta_units[b+1]); nullptr: unit b
+  const float* binv;     // node-block Jacobi sweeps: per node 3x3 inverse diagonal block
+                         // [xx, yy, zz, xy, xz, yz]; nullptr: point Jacobi with invd
 };
 
 template <typename T>
@@ -202,12 +204,18 @@ stencil_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
       }
     } else {
       const bool pin = (pg + col0 == 0);
+      T dv[3];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if (OUT == OUT_RESID) {
-          st_val(ob + c * st, pin ? (T)0 : eb[c] - y[c]);
-        } else {
-          const T xv = unode[c] + (T)a.omega * eid * (eb[c] - y[c]);
+      for (int c = 0; c < 3; ++c) dv[c] = eb[c] - y[c];
+      if (OUT == OUT_RESID) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) st_val(ob + c * st, pin ? (T)0 : dv[c]);
+      } else {
+        jacobi_dir<T>(a.binv, cd.off + pg + col0, (T)a.omega * eid, dv);   // point: omega invd folded in
+        const T sc = a.binv ? (T)a.omega : (T)1;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const T xv = unode[c] + sc * dv[c];
           st_val(ob + c * st, xv);
           if (OUT == OUT_JACOBI_DOT) acc += (double)xv * (double)eb[c];
         }
@@ -421,12 +429,18 @@ stencil2_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
       }
     } else {
       const bool pin = (node == 0);
+      T dv[3];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if (OUT == OUT_RESID) {
-          st_val(ob + c * st, pin ? (T)0 : ebv[c] - y[c]);
-        } else {
-          const T xv = un_[c] + (T)a.omega * idv * (ebv[c] - y[c]);
+      for (int c = 0; c < 3; ++c) dv[c] = ebv[c] - y[c];
+      if (OUT == OUT_RESID) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) st_val(ob + c * st, pin ? (T)0 : dv[c]);
+      } else {
+        jacobi_dir<T>(a.binv, cd.off + node, (T)a.omega * idv, dv);   // point: omega invd folded in
+        const T sc = a.binv ? (T)a.omega : (T)1;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const T xv = un_[c] + sc * dv[c];
           st_val(ob + c * st, xv);
           if (OUT == OUT_JACOBI_DOT) acc += (double)xv * (double)ebv[c];
         }
@@ -606,6 +620,20 @@ __device__ __forceinline__ f2 p_sub(f2 a, f2 b) {
 }
 __device__ __forceinline__ f2 p_bc(float s) { return make_float2(s, s); }
 
+// Node-block Jacobi direction of two nodes in the two lanes: d <- B d with
+// lane x the block at b1, lane y the block at b2 (layout of jacobi_dir).
+__device__ __forceinline__ void block_dir2(const float* __restrict__ b1, const float* __restrict__ b2, f2 (&d)[3]) {
+  const float2 p01 = *reinterpret_cast<const float2*>(b1), q01 = *reinterpret_cast<const float2*>(b2);
+  const float2 p23 = *reinterpret_cast<const float2*>(b1 + 2), q23 = *reinterpret_cast<const float2*>(b2 + 2);
+  const float2 p45 = *reinterpret_cast<const float2*>(b1 + 4), q45 = *reinterpret_cast<const float2*>(b2 + 4);
+  const f2 xx = make_float2(p01.x, q01.x), yy = make_float2(p01.y, q01.y), zz = make_float2(p23.x, q23.x);
+  const f2 xy = make_float2(p23.y, q23.y), xz = make_float2(p45.x, q45.x), yz = make_float2(p45.y, q45.y);
+  const f2 d0 = d[0], d1 = d[1], d2 = d[2];
+  d[0] = p_fma(xz, d2, p_fma(xy, d1, p_mul(xx, d0)));
+  d[1] = p_fma(yz, d2, p_fma(yy, d1, p_mul(xy, d0)));
+  d[2] = p_fma(zz, d2, p_fma(yz, d1, p_mul(xz, d0)));
+}
+
 // 2x2 Hadamard transform of a node patch, index 2*ay + az (same stage order
 // and signs as fwht8_fwd restricted to bits 1 and 2).
 __device__ __forceinline__ void had4_fwd(f2 (&v)[4]) {
@@ -777,6 +805,19 @@ stencilp_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
     } else {
       const bool pin = (pg + col0 == 0);
       const f2 wd = p_bc((float)a.omega * eid);
+      f2 bd[3];   // node-block Jacobi: omega B (b - y), both load cases
+      if (OUT != OUT_RESID && a.binv) {
+        float dA[3], dB[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          dA[c] = (float)ebA[c] - y[c].x;
+          dB[c] = (float)ebB[c] - y[c].y;
+        }
+        jacobi_dir<float>(a.binv, cd.off + pg + col0, 0.f, dA);
+        jacobi_dir<float>(a.binv, cd.off + pg + col0, 0.f, dB);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) bd[c] = p_mul(p_bc((float)a.omega), make_float2(dA[c], dB[c]));
+      }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const f2 bv = make_float2((float)ebA[c], (float)ebB[c]);
@@ -785,7 +826,7 @@ stencilp_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
           st_val(ob + c * st, pin ? 0.f : d.x);
           st_val(ob + c * st + st3, pin ? 0.f : d.y);
         } else {
-          const f2 xv = p_fma(wd, d, unode[c]);
+          const f2 xv = a.binv ? p_add(unode[c], bd[c]) : p_fma(wd, d, unode[c]);
           st_val(ob + c * st, xv.x);
           st_val(ob + c * st + st3, xv.y);
           if (OUT == OUT_JACOBI_DOT) {
@@ -1049,6 +1090,12 @@ stencil2p_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
     } else {
       const bool pin1 = (pg + c1 == 0), pin2 = (pg + c2 == 0);
       const f2 wd = p_mul(p_bc((float)a.omega), id12);
+      f2 bd[3];   // node-block Jacobi: B (b - y) of both nodes
+      if (OUT != OUT_RESID && a.binv) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) bd[c] = p_sub(make_float2((float)eb1[c], (float)eb2[c]), y[c]);
+        block_dir2(a.binv + 6 * (cd.off + pg + c1), a.binv + 6 * (cd.off + pg + c2), bd);
+      }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const f2 bv = make_float2((float)eb1[c], (float)eb2[c]);
@@ -1057,7 +1104,7 @@ stencil2p_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
           if (own1) st_val(ob + c * st + c1, pin1 ? 0.f : d.x);
           if (own2) st_val(ob + c * st + c2, pin2 ? 0.f : d.y);
         } else {
-          const f2 xv = p_fma(wd, d, u12[c]);
+          const f2 xv = a.binv ? p_fma(p_bc((float)a.omega), bd[c], u12[c]) : p_fma(wd, d, u12[c]);
           if (own1) st_val(ob + c * st + c1, xv.x);
           if (own2) st_val(ob + c * st + c2, xv.y);
           if (OUT == OUT_JACOBI_DOT) {
@@ -1298,8 +1345,10 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
   const int zm = (z == 0) ? nz - 1 : z - 1;
 
   constexpr int RB = 2 * TR - 1, NRU = RB + 3, NRK = RB + 2;
+  // stage layout (floats): U[3][NRU][nz], KC[NRK][nz], B[3][RB][nz], I[RB][nz][6]
+  // (invd rows, or the node-block inverses [6] of a block sweep)
   constexpr int oK = 3 * NRU * NZ, oB = oK + NRK * NZ, oI = oB + 3 * RB * NZ;
-  constexpr int SS = (oI + RB * NZ + 3) & ~3;
+  constexpr int SS = (oI + 6 * RB * NZ + 3) & ~3;
   constexpr int PS = TR * 3 * nz;
   float* stg = reinterpret_cast<float*>(smem_raw);
   f2* QAB = reinterpret_cast<f2*>(stg + kBulkSlots * SS);   // [2][TR][3][nz]
@@ -1345,11 +1394,12 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
     float* obase = a.out + (long long)rhs * 3 * st + cd.off;
 
     const char* src_base = nullptr;
-    int plane_lag = 0, src_off = 0, dst_off = 0, bytes = 0;
+    int plane_lag = 0, src_off = 0, dst_off = 0, bytes = 0, esz = 4;
     unsigned tx_total = 0;
     if (tid < 32) {
       int idx = 0;
-      auto seg = [&](const float* base, int lag, int row0, int nrows, int dst) {
+      // es: bytes per node of the array (4, or 24 for the node blocks)
+      auto seg = [&](const float* base, int lag, int row0, int nrows, int dst, int es = 4) {
         int done = 0;
         while (done < nrows) {
           const int r0 = wrapy(row0 + done);
@@ -1357,11 +1407,12 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
           if (idx == tid) {
             src_base = reinterpret_cast<const char*>(base);
             plane_lag = lag;
+            esz = es;
             src_off = r0 * nz;
-            dst_off = dst + done * nz;
-            bytes = n * nz * 4;
+            dst_off = dst + done * nz * (es / 4);
+            bytes = n * nz * es;
           }
-          tx_total += (unsigned)(n * nz * 4);
+          tx_total += (unsigned)(n * nz * es);
           ++idx;
           done += n;
         }
@@ -1372,7 +1423,10 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
       if (OUT >= OUT_JACOBI) {
         for (int c = 0; c < 3; ++c)
           seg(a.b + ((long long)rhs * 3 + c) * st + cd.off, -1, un.j0, rows, oB + c * RB * nz);
-        if (OUT != OUT_RESID) seg(a.invd + cd.off, -1, un.j0, rows, oI);
+        if (OUT != OUT_RESID) {
+          if (a.binv) seg(a.binv + 6 * cd.off, -1, un.j0, rows, oI, 24);
+          else seg(a.invd + cd.off, -1, un.j0, rows, oI);
+        }
       }
     }
     int pl_next = ((un.i0 - 2 + plane_lag) % nx + nx) % nx;
@@ -1388,8 +1442,8 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
       }
       __syncwarp();
       if (bytes > 0)
-        bulk_g2s(smem_addr(stg + slot * SS + dst_off), src_base + 4LL * ((long long)pl_next * plane + src_off),
-                 (unsigned)bytes, bar);
+        bulk_g2s(smem_addr(stg + slot * SS + dst_off),
+                 src_base + (long long)esz * ((long long)pl_next * plane + src_off), (unsigned)bytes, bar);
       if (++pl_next == nx) pl_next = 0;
     };
     const int G = len + 3;
@@ -1453,9 +1507,19 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
         const bool pin1 = (pg + c1 == 0), pin2 = (pg + c2 == 0);
         const float* Bs = S + oB;
         f2 wd = p_bc(0.f);
+        f2 bd[3];   // node-block sweep: omega B (b - y) of both nodes (rows beyond the tile are not stored)
         if (OUT != OUT_RESID) {
           const float* Is = S + oI;
-          wd = p_mul(p_bc((float)a.omega), make_float2(own1 ? Is[r1] : 0.f, own2 ? Is[r2] : 0.f));
+          if (a.binv) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+              bd[c] = p_sub(make_float2(Bs[c * RB * NZ + r1], Bs[c * RB * NZ + r2]), y[c]);
+            block_dir2(Is + 6 * r1, Is + 6 * r2, bd);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) bd[c] = p_mul(p_bc((float)a.omega), bd[c]);
+          } else {
+            wd = p_mul(p_bc((float)a.omega), make_float2(own1 ? Is[r1] : 0.f, own2 ? Is[r2] : 0.f));
+          }
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -1465,7 +1529,7 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
             if (own1) ob[c * st + c1] = pin1 ? 0.f : d.x;
             if (own2) ob[c * st + c2] = pin2 ? 0.f : d.y;
           } else {
-            const f2 xv = p_fma(wd, d, u12[c]);
+            const f2 xv = a.binv ? p_add(u12[c], bd[c]) : p_fma(wd, d, u12[c]);
             if (own1) ob[c * st + c1] = xv.x;
             if (own2) ob[c * st + c2] = xv.y;
             if (OUT == OUT_JACOBI_DOT) {
@@ -1688,7 +1752,7 @@ stencil1b_kernel(StencilArgs<TIn, double, double, double> a) {
     seg(a.kc + cd.off, 8, 0, un.j0 - 1, rows + 1, bK);
     if (OUT >= OUT_JACOBI) {
       for (int c = 0; c < 3; ++c) seg(a.b + ((long long)rhs * 3 + c) * st + cd.off, 8, -1, un.j0, rows, bB + c * RB * nz * 8);
-      if (OUT != OUT_RESID) seg(a.invd + cd.off, 4, -1, un.j0, rows, bI);
+      if (OUT != OUT_RESID && !a.binv) seg(a.invd + cd.off, 4, -1, un.j0, rows, bI);
     }
   }
   int pl_next = ((un.i0 - 2 + plane_lag) % nx + nx) % nx;
@@ -1748,25 +1812,39 @@ stencil1b_kernel(StencilArgs<TIn, double, double, double> a) {
     double* ob = obase + pg + col;
     const int rb = (r - 1) * nz + z;   // owned row in the b / invd arrays
     const bool pin = (pg + col == 0);
-    double idv = 0.0;
-    if (OUT == OUT_JACOBI || OUT == OUT_JACOBI_DOT) idv = (double)reinterpret_cast<const float*>(S + bI)[rb];
     const double* Bs = reinterpret_cast<const double*>(S + bB);
+    double y[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const double y = own[c] + Qg[qrow + (0 * 3 + c) * nz + zm] + Qg[qup + (1 * 3 + c) * nz + z] +
-                       Qg[qup + (2 * 3 + c) * nz + zm];
-      if (OUT == OUT_APPLY || OUT == OUT_APPLY_DOT) {
-        ob[c * st] = y;
-        if (OUT == OUT_APPLY_DOT) acc += unode[c] * y;
+    for (int c = 0; c < 3; ++c)
+      y[c] = own[c] + Qg[qrow + (0 * 3 + c) * nz + zm] + Qg[qup + (1 * 3 + c) * nz + z] + Qg[qup + (2 * 3 + c) * nz + zm];
+    if (OUT == OUT_APPLY || OUT == OUT_APPLY_DOT) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ob[c * st] = y[c];
+        if (OUT == OUT_APPLY_DOT) acc += unode[c] * y[c];
+      }
+    } else if (OUT == OUT_RESID) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ob[c * st] = pin ? 0.0 : Bs[c * RB * nz + rb] - y[c];
+    } else {
+      const float* Is = reinterpret_cast<const float*>(S + bI);
+      double dv[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) dv[c] = Bs[c * RB * nz + rb] - y[c];
+      if (a.binv) {   // node-block sweep: the node's block inverse, read where the gather needs it
+        jacobi_dir<double>(a.binv, cd.off + pg + col, 0.0, dv);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dv[c] *= a.omega;
       } else {
-        const double bv = Bs[c * RB * nz + rb];
-        if (OUT == OUT_RESID) {
-          ob[c * st] = pin ? 0.0 : bv - y;
-        } else {
-          const double xv = unode[c] + a.omega * idv * (bv - y);
-          ob[c * st] = xv;
-          if (OUT == OUT_JACOBI_DOT) acc += xv * bv;
-        }
+        const double idv = a.omega * (double)Is[rb];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dv[c] *= idv;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double xv = unode[c] + dv[c];
+        ob[c * st] = xv;
+        if (OUT == OUT_JACOBI_DOT) acc += xv * Bs[c * RB * nz + rb];
       }
     }
   };
@@ -1857,7 +1935,7 @@ inline size_t stencil1b_smem_bytes(int NT, int nz, int in_size) {
 // Shared memory bytes of one stencil2b_kernel CTA (tiles of up to 2*TR-1 rows).
 inline size_t stencil2b_smem_bytes(int NT, int nz) {
   const int TR = NT / nz, rows = 2 * TR - 1;
-  const size_t SS = ((size_t)(3 * (rows + 3) + (rows + 2) + 4 * rows) * nz + 3) & ~(size_t)3;   // as in the kernel
+  const size_t SS = ((size_t)(3 * (rows + 3) + (rows + 2) + 9 * rows) * nz + 3) & ~(size_t)3;   // as in the kernel
   return sizeof(float) * kBulkSlots * SS + sizeof(f2) * 4 * (size_t)TR * 3 * nz +
          sizeof(unsigned long long) * kBulkSlots + 64 * sizeof(double);
 }

@@ -104,8 +104,13 @@ typedef struct {
   double cheb_ratio;      /* 0: every smoothing sweep is damped by omega; > 1: the sweeps
                              of a pass use the reciprocal roots of the Chebyshev
                              polynomial of that degree on [lmax/cheb_ratio, lmax], lmax =
-                             the largest eigenvalue of diag(K0)^-1 K0 (a bound on the
-                             spectrum of D^-1 K for every coefficient field) */
+                             the largest eigenvalue of D0^-1 K0 (a bound on the spectrum
+                             of D^-1 K for every coefficient field; D0 the element's
+                             diagonal, or its 3x3 node blocks with block_jacobi) */
+  int block_jacobi;       /* multigrid sweeps: 0 point Jacobi, D = diag(K); 1 node-block
+                             Jacobi, D = the 3x3 diagonal blocks of K (the three
+                             displacement components of a node solved together; they
+                             couple where the coefficients jump) */
 } femh_config;
 
 typedef struct {

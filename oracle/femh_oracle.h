@@ -39,6 +39,10 @@ int fo_num_threads(void);
 int fo_mg_homogenize(int nx, int ny, int nz, double h, const double* rho, const fo_material* m,
                      double tol, int max_iter, int pre, int post, double cheb_ratio, int coarse_max,
                      double C[36], double* chi_out, int iters[6], double rel[6]);
+/* the same with the node-block Jacobi smoother when block != 0 */
+int fo_mg_homogenize_b(int nx, int ny, int nz, double h, const double* rho, const fo_material* m,
+                       double tol, int max_iter, int pre, int post, double cheb_ratio, int coarse_max,
+                       int block, double C[36], double* chi_out, int iters[6], double rel[6]);
 void fo_mg_apply(int nx, int ny, int nz, double h, const double* coef, double nu, const double* u,
                  double* y);
 

@@ -57,6 +57,7 @@ typedef struct {
   long nv;
   double* kc;     /* [nv] modulus x voxel edge: the voxel's K0(1) multiplier */
   double* dinv;   /* [3][nv] inverse operator diagonal, 0 at node 0 */
+  double* binv;   /* node-block smoother: [nv][6] inverse 3x3 diagonal blocks (xx yy zz xy xz yz), or NULL */
   double* x;      /* [6][3][nv] */
   double* b;
   double* t;
@@ -70,6 +71,7 @@ typedef struct {
   hadk_t hk;
   double K0[576];   /* K0(1) */
   int pre, post;
+  int block;        /* node-block Jacobi sweeps */
   double wpre[16], wpost[16];
 } mg_t;
 
@@ -253,24 +255,62 @@ static void mg_apply(const mglev_t* L, const hadk_t* H, const double* u, double*
 }
 
 /* ------------------------------------------------------------- levels --- */
-static double lmax_bound(const double K0[576]) {
-  /* largest eigenvalue of D^-1/2 K0 D^-1/2 by power iteration (symmetric PSD) */
+static double lmax_bound(const double K0[576], int block) {
+  /* largest eigenvalue of D^-1 K0 (D the diagonal, or with block the 3x3 node
+     blocks) by power iteration on the symmetric L^-1 K0 L^-T, L = chol(D) */
+  double Li[576];
+  memset(Li, 0, sizeof(Li));
+  for (int a = 0; a < 8; ++a) {
+    if (!block) {
+      for (int c = 0; c < 3; ++c) Li[(3 * a + c) * 25] = 1.0 / sqrt(K0[(3 * a + c) * 25]);
+      continue;
+    }
+    double L[3][3] = {{0}}, I[3][3] = {{0}};
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j <= i; ++j) {
+        double v = K0[(3 * a + i) * 24 + 3 * a + j];
+        for (int k = 0; k < j; ++k) v -= L[i][k] * L[j][k];
+        L[i][j] = (i == j) ? sqrt(v) : v / L[j][j];
+      }
+    for (int c = 0; c < 3; ++c)
+      for (int i = 0; i < 3; ++i) {
+        double v = (i == c) ? 1.0 : 0.0;
+        for (int k = 0; k < i; ++k) v -= L[i][k] * I[k][c];
+        I[i][c] = v / L[i][i];
+      }
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) Li[(3 * a + i) * 24 + 3 * a + j] = I[i][j];
+  }
+  double S[576], T[576];
+  for (int i = 0; i < 24; ++i)
+    for (int j = 0; j < 24; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < 24; ++k) v += Li[i * 24 + k] * K0[k * 24 + j];
+      T[i * 24 + j] = v;
+    }
+  for (int i = 0; i < 24; ++i)
+    for (int j = 0; j < 24; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < 24; ++k) v += T[i * 24 + k] * Li[j * 24 + k];
+      S[i * 24 + j] = v;
+    }
   double x[24], y[24];
   for (int p = 0; p < 24; ++p) x[p] = 1.0 + 0.01 * p;
   double lam = 0.0;
   for (int it = 0; it < 2000; ++it) {
     double nrm = 0.0;
     for (int p = 0; p < 24; ++p) {
-      double s = 0.0;
-      for (int q = 0; q < 24; ++q) s += K0[p * 24 + q] / sqrt(K0[p * 25] * K0[q * 25]) * x[q];
-      y[p] = s;
-      nrm += s * s;
+      double sacc = 0.0;
+      for (int q = 0; q < 24; ++q) sacc += S[p * 24 + q] * x[q];
+      y[p] = sacc;
+      nrm += sacc * sacc;
     }
     nrm = sqrt(nrm);
-    double dotv = 0.0;
-    for (int p = 0; p < 24; ++p) dotv += x[p] * y[p];
-    double xn = 0.0;
-    for (int p = 0; p < 24; ++p) xn += x[p] * x[p];
+    double dotv = 0.0, xn = 0.0;
+    for (int p = 0; p < 24; ++p) {
+      dotv += x[p] * y[p];
+      xn += x[p] * x[p];
+    }
     lam = dotv / xn;
     for (int p = 0; p < 24; ++p) x[p] = y[p] / nrm;
   }
@@ -303,6 +343,67 @@ static void level_diag(mglev_t* L, const double K0[576]) {
       for (int c = 0; c < 3; ++c) acc[c] += L->kc[e] * K0[(3 * a + c) * 25];
     }
     for (int c = 0; c < 3; ++c) L->dinv[(long)c * nv + n] = n == 0 ? 0.0 : 1.0 / acc[c];
+  }
+}
+
+/* node-block smoother: D_n = sum over the 8 voxels at n of kc_e K0_aa (the
+   3x3 diagonal block of K at n), inverted; 0 at node 0 */
+static void level_block(mglev_t* L, const double K0[576]) {
+  const long nv = L->nv;
+  const int nx = L->nx, ny = L->ny, nz = L->nz;
+#pragma omp parallel for schedule(static)
+  for (long n = 0; n < nv; ++n) {
+    const int i = (int)(n / ((long)ny * nz)), j = (int)((n / nz) % ny), k = (int)(n % nz);
+    double D[3][3] = {{0}};
+    for (int a = 0; a < 8; ++a) {
+      const long e = ((long)wrapi(i - ((a >> 2) & 1), nx) * ny + wrapi(j - ((a >> 1) & 1), ny)) * nz +
+                     wrapi(k - (a & 1), nz);
+      for (int c1 = 0; c1 < 3; ++c1)
+        for (int c2 = 0; c2 < 3; ++c2) D[c1][c2] += L->kc[e] * K0[(3 * a + c1) * 24 + 3 * a + c2];
+    }
+    double* o = L->binv + 6 * n;
+    if (n == 0) {
+      for (int q = 0; q < 6; ++q) o[q] = 0.0;
+      continue;
+    }
+    const double c00 = D[1][1] * D[2][2] - D[1][2] * D[2][1], c01 = D[1][2] * D[2][0] - D[1][0] * D[2][2],
+                 c02 = D[1][0] * D[2][1] - D[1][1] * D[2][0];
+    const double det = D[0][0] * c00 + D[0][1] * c01 + D[0][2] * c02;
+    o[0] = c00 / det;
+    o[1] = (D[0][0] * D[2][2] - D[0][2] * D[2][0]) / det;
+    o[2] = (D[0][0] * D[1][1] - D[0][1] * D[1][0]) / det;
+    o[3] = c01 / det;
+    o[4] = c02 / det;
+    o[5] = (D[0][2] * D[1][0] - D[0][0] * D[1][2]) / det;
+  }
+}
+
+/* x (+)= w D^-1 v for the 3 components of every node: v = b - t, or b alone
+   when t == NULL (with from_zero the sweep starts x from zero) */
+static void block_sweep(const mglev_t* L, double* x, const double* b, const double* t, double w, int from_zero) {
+  const long nv = L->nv;
+#pragma omp parallel for schedule(static)
+  for (long rn = 0; rn < 6 * nv; ++rn) {
+    const long rr = rn / nv, n = rn % nv;
+    const double* B = L->binv + 6 * n;
+    double v[3];
+    for (int c = 0; c < 3; ++c) {
+      const long q = (rr * 3 + c) * nv + n;
+      v[c] = t ? b[q] - t[q] : b[q];
+    }
+    const double d0 = B[0] * v[0] + B[3] * v[1] + B[4] * v[2];
+    const double d1 = B[3] * v[0] + B[1] * v[1] + B[5] * v[2];
+    const double d2 = B[4] * v[0] + B[5] * v[1] + B[2] * v[2];
+    const long q0 = (rr * 3) * nv + n;
+    if (from_zero) {
+      x[q0] = w * d0;
+      x[q0 + nv] = w * d1;
+      x[q0 + 2 * nv] = w * d2;
+    } else {
+      x[q0] += w * d0;
+      x[q0 + nv] += w * d1;
+      x[q0 + 2 * nv] += w * d2;
+    }
   }
 }
 
@@ -417,6 +518,10 @@ static void prolong_add(const mglev_t* F, const mglev_t* C, double* xf, const do
 
 /* x += w D^-1 (b - t) */
 static void jacobi_update(const mglev_t* L, double* x, const double* b, const double* t, double w) {
+  if (L->binv) {
+    block_sweep(L, x, b, t, w, 0);
+    return;
+  }
   const long nv = L->nv;
 #pragma omp parallel for schedule(static)
   for (long q = 0; q < 18 * nv; ++q) {
@@ -433,8 +538,12 @@ static void vcycle(mg_t* M, int l) {
     return;
   }
   /* first pre-sweep from x = 0 */
+  if (L->binv) {
+    block_sweep(L, L->x, L->b, NULL, M->wpre[0], 1);
+  } else {
 #pragma omp parallel for schedule(static)
-  for (long q = 0; q < n18; ++q) L->x[q] = M->wpre[0] * L->dinv[q % (3 * L->nv)] * L->b[q];
+    for (long q = 0; q < n18; ++q) L->x[q] = M->wpre[0] * L->dinv[q % (3 * L->nv)] * L->b[q];
+  }
   for (int s = 1; s < M->pre; ++s) {
     mg_apply(L, &M->hk, L->x, L->t);
     jacobi_update(L, L->x, L->b, L->t, M->wpre[s]);
@@ -456,6 +565,7 @@ static void mg_free(mg_t* M) {
   for (int l = 0; l < M->nlev; ++l) {
     free(M->lv[l].kc);
     free(M->lv[l].dinv);
+    free(M->lv[l].binv);
     free(M->lv[l].x);
     free(M->lv[l].b);
     free(M->lv[l].t);
@@ -465,13 +575,14 @@ static void mg_free(mg_t* M) {
 }
 
 static int mg_setup(mg_t* M, int nx, int ny, int nz, double h, const double* coef, int pre, int post,
-                    double ratio, int coarse_max, double nu) {
+                    double ratio, int coarse_max, double nu, int block) {
   memset(M, 0, sizeof(*M));
   fo_k0(1.0, nu, 1.0, M->K0);
   hadamard_k(M->K0, &M->hk);
   M->pre = pre < 1 ? 1 : (pre > 16 ? 16 : pre);
   M->post = post < 0 ? 0 : (post > 16 ? 16 : post);
-  const double lmax = lmax_bound(M->K0);
+  M->block = block != 0;
+  const double lmax = lmax_bound(M->K0, M->block);
   weights(M->pre, lmax, ratio, M->wpre);
   double wp[16];
   weights(M->post, lmax, ratio, wp);
@@ -485,6 +596,7 @@ static int mg_setup(mg_t* M, int nx, int ny, int nz, double h, const double* coe
     L->nv = (long)dims[0] * dims[1] * dims[2];
     L->kc = (double*)malloc(sizeof(double) * L->nv);
     L->dinv = (double*)malloc(sizeof(double) * 3 * L->nv);
+    L->binv = M->block ? (double*)malloc(sizeof(double) * 6 * L->nv) : NULL;
     L->x = (double*)calloc(18 * L->nv, sizeof(double));
     L->b = (double*)calloc(18 * L->nv, sizeof(double));
     L->t = (double*)calloc(18 * L->nv, sizeof(double));
@@ -503,6 +615,7 @@ static int mg_setup(mg_t* M, int nx, int ny, int nz, double h, const double* coe
       }
     }
     level_diag(L, M->K0);
+    if (L->binv) level_block(L, M->K0);
     const int halve = L->nv > coarse_max && dims[0] % 2 == 0 && dims[1] % 2 == 0 && dims[2] % 2 == 0 &&
                       dims[0] >= 4 && dims[1] >= 4 && dims[2] >= 4 && l + 1 < MAXLEV;
     if (!halve) break;
@@ -563,13 +676,20 @@ static void mg_rhs(const mglev_t* L, const double K0[576], double h, double* b) 
 int fo_mg_homogenize(int nx, int ny, int nz, double h, const double* rho, const fo_material* mat, double tol,
                      int max_iter, int pre, int post, double cheb_ratio, int coarse_max, double C[36],
                      double* chi_out, int iters[6], double rel[6]) {
+  return fo_mg_homogenize_b(nx, ny, nz, h, rho, mat, tol, max_iter, pre, post, cheb_ratio, coarse_max, 0, C,
+                            chi_out, iters, rel);
+}
+
+int fo_mg_homogenize_b(int nx, int ny, int nz, double h, const double* rho, const fo_material* mat, double tol,
+                       int max_iter, int pre, int post, double cheb_ratio, int coarse_max, int block, double C[36],
+                       double* chi_out, int iters[6], double rel[6]) {
   const long nv = (long)nx * ny * nz;
   const long n3 = 3 * nv, n18 = 18 * nv;
   if (nx < 2 || ny < 2 || nz < 2 || nz > 256) return -2;
   double* coef = (double*)malloc(sizeof(double) * nv);
   for (long e = 0; e < nv; ++e) coef[e] = fo_coef(mat, rho[e]);
   mg_t* M = (mg_t*)malloc(sizeof(mg_t));
-  if (mg_setup(M, nx, ny, nz, h, coef, pre, post, cheb_ratio, coarse_max, mat->nu) != 0) {
+  if (mg_setup(M, nx, ny, nz, h, coef, pre, post, cheb_ratio, coarse_max, mat->nu, block) != 0) {
     free(coef);
     free(M);
     return -3;

@@ -72,6 +72,10 @@ def lib():
             ctypes.c_double, dp, ctypes.POINTER(Material), ctypes.c_double, ctypes.c_int, ctypes.c_int,
             ctypes.c_int, ctypes.c_double, ctypes.c_int, dp, dp, ctypes.POINTER(ctypes.c_int), dp]
         L.fo_mg_homogenize.restype = ctypes.c_int
+        L.fo_mg_homogenize_b.argtypes = [ctypes.c_int] * 3 + [
+            ctypes.c_double, dp, ctypes.POINTER(Material), ctypes.c_double, ctypes.c_int, ctypes.c_int,
+            ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, dp, dp, ctypes.POINTER(ctypes.c_int), dp]
+        L.fo_mg_homogenize_b.restype = ctypes.c_int
         L.fo_mg_apply.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double, dp, ctypes.c_double, dp, dp]
         _lib = L
     return _lib
@@ -131,10 +135,10 @@ def homogenize(rho: np.ndarray, h: float | None = None, mat: Material | None = N
 
 def mg_homogenize(rho: np.ndarray, h: float | None = None, mat: Material | None = None,
                   tol: float = 1e-10, max_iter: int = 2000, pre: int = 3, post: int = 3,
-                  cheb_ratio: float = 64.0, coarse_max: int = 64, want_chi: bool = True):
+                  cheb_ratio: float = 64.0, coarse_max: int = 64, want_chi: bool = True, block: bool = False):
     """Same problem and outputs as ``homogenize``, solved by the multigrid PCG of
-    femh_oracle_mg.c.  Returns (C[6,6], chi[6,nx,ny,nz,3] or None, iters[6],
-    rel[6], status)."""
+    femh_oracle_mg.c (point-Jacobi sweeps, or node-block Jacobi with block).
+    Returns (C[6,6], chi[6,nx,ny,nz,3] or None, iters[6], rel[6], status)."""
     rho = np.ascontiguousarray(rho, dtype=np.float64)
     nx, ny, nz = rho.shape
     if h is None:
@@ -145,8 +149,9 @@ def mg_homogenize(rho: np.ndarray, h: float | None = None, mat: Material | None 
     chi = np.zeros((6, nx, ny, nz, 3)) if want_chi else None
     iters = (ctypes.c_int * 6)()
     rel = np.zeros(6)
-    st = lib().fo_mg_homogenize(nx, ny, nz, h, _p(rho), ctypes.byref(mat), tol, max_iter, pre, post,
-                                cheb_ratio, coarse_max, _p(C), _p(chi) if want_chi else None, iters, _p(rel))
+    st = lib().fo_mg_homogenize_b(nx, ny, nz, h, _p(rho), ctypes.byref(mat), tol, max_iter, pre, post,
+                                  cheb_ratio, coarse_max, 1 if block else 0, _p(C), _p(chi) if want_chi else None,
+                                  iters, _p(rel))
     return C, chi, list(iters), rel, st
 
 

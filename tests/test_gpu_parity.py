@@ -168,6 +168,27 @@ def test_chebyshev_smoother_C_matches_oracle(femh, oracle, precision, smoothing)
     assert _rel(C, Co) < (TOL_FP64 if precision == "fp64" else TOL_MIXED)
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("precision", ["fp64", "mixed_pc"])
+def test_block_jacobi_C_matches_oracle(femh, oracle, precision, variant):
+    """Node-block Jacobi sweeps (block_jacobi=1: every node's 3x3 diagonal
+    block of K inverted, the Chebyshev interval from the block-scaled element
+    bound) through each stencil kernel forced in turn (0: the autotuner's
+    choice; runtime-z kernels on the coarse levels 12^3 and below) reach the
+    oracle's C^H on a 24^3 binary cell, in fewer iterations than point sweeps."""
+    from fem_b200 import fields
+    rho = fields.binary_cell(24, 0.4, seed=4)
+    Co = _oracle_C(oracle, "binary24", rho)
+    prec = {"fp64": femh.FP64, "mixed_pc": femh.MIXED_PC}[precision]
+    e = femh.Engine(precision=prec, block_jacobi=1, stencil_variant=variant, autotune=1 if variant == 0 else 0)
+    C, info = e.homogenize(rho)
+    assert info["status"] == 0 and max(info["rel_residual"]) < 1e-10
+    assert _rel(C, Co) < (TOL_FP64 if precision == "fp64" else TOL_MIXED)
+    if variant == 0:
+        _, ip = femh.Engine(precision=prec, block_jacobi=0).homogenize(rho)
+        assert max(info["iterations"]) < max(ip["iterations"])
+
+
 _ORACLE_C = {}
 
 
