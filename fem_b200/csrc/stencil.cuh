@@ -805,7 +805,7 @@ stencilp_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
     } else {
       const bool pin = (pg + col0 == 0);
       const f2 wd = p_bc((float)a.omega * eid);
-      f2 bd[3];   // node-block Jacobi: omega B (b - y), both load cases
+      f2 bd[3];   // node-block Jacobi: B (b - y), both load cases
       if (OUT != OUT_RESID && a.binv) {
         float dA[3], dB[3];
 #pragma unroll
@@ -816,7 +816,7 @@ stencilp_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
         jacobi_dir<float>(a.binv, cd.off + pg + col0, 0.f, dA);
         jacobi_dir<float>(a.binv, cd.off + pg + col0, 0.f, dB);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) bd[c] = p_mul(p_bc((float)a.omega), make_float2(dA[c], dB[c]));
+        for (int c = 0; c < 3; ++c) bd[c] = make_float2(dA[c], dB[c]);
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -826,7 +826,7 @@ stencilp_kernel(StencilArgs<TIn, TOut, TB, TC> a) {
           st_val(ob + c * st, pin ? 0.f : d.x);
           st_val(ob + c * st + st3, pin ? 0.f : d.y);
         } else {
-          const f2 xv = a.binv ? p_add(unode[c], bd[c]) : p_fma(wd, d, unode[c]);
+          const f2 xv = a.binv ? p_fma(p_bc((float)a.omega), bd[c], unode[c]) : p_fma(wd, d, unode[c]);
           st_val(ob + c * st, xv.x);
           st_val(ob + c * st + st3, xv.y);
           if (OUT == OUT_JACOBI_DOT) {
@@ -1507,7 +1507,7 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
         const bool pin1 = (pg + c1 == 0), pin2 = (pg + c2 == 0);
         const float* Bs = S + oB;
         f2 wd = p_bc(0.f);
-        f2 bd[3];   // node-block sweep: omega B (b - y) of both nodes (rows beyond the tile are not stored)
+        f2 bd[3];   // node-block sweep: B (b - y) of both nodes (rows beyond the tile are not stored)
         if (OUT != OUT_RESID) {
           const float* Is = S + oI;
           if (a.binv) {
@@ -1515,8 +1515,6 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
             for (int c = 0; c < 3; ++c)
               bd[c] = p_sub(make_float2(Bs[c * RB * NZ + r1], Bs[c * RB * NZ + r2]), y[c]);
             block_dir2(Is + 6 * r1, Is + 6 * r2, bd);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) bd[c] = p_mul(p_bc((float)a.omega), bd[c]);
           } else {
             wd = p_mul(p_bc((float)a.omega), make_float2(own1 ? Is[r1] : 0.f, own2 ? Is[r2] : 0.f));
           }
@@ -1529,7 +1527,7 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
             if (own1) ob[c * st + c1] = pin1 ? 0.f : d.x;
             if (own2) ob[c * st + c2] = pin2 ? 0.f : d.y;
           } else {
-            const f2 xv = a.binv ? p_add(u12[c], bd[c]) : p_fma(wd, d, u12[c]);
+            const f2 xv = a.binv ? p_fma(p_bc((float)a.omega), bd[c], u12[c]) : p_fma(wd, d, u12[c]);
             if (own1) ob[c * st + c1] = xv.x;
             if (own2) ob[c * st + c2] = xv.y;
             if (OUT == OUT_JACOBI_DOT) {
