@@ -1506,33 +1506,36 @@ stencil2b_kernel(StencilArgs<float, float, float, float> a) {
       } else {
         const bool pin1 = (pg + c1 == 0), pin2 = (pg + c2 == 0);
         const float* Bs = S + oB;
-        f2 wd = p_bc(0.f);
-        f2 bd[3];   // node-block sweep: B (b - y) of both nodes (rows beyond the tile are not stored)
-        if (OUT != OUT_RESID) {
-          const float* Is = S + oI;
-          if (a.binv) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-              bd[c] = p_sub(make_float2(Bs[c * RB * NZ + r1], Bs[c * RB * NZ + r2]), y[c]);
-            block_dir2(Is + 6 * r1, Is + 6 * r2, bd);
-          } else {
-            wd = p_mul(p_bc((float)a.omega), make_float2(own1 ? Is[r1] : 0.f, own2 ? Is[r2] : 0.f));
-          }
-        }
+        // rows beyond the tile read stale stage entries: their lanes are not stored
+        f2 bv[3], d[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const f2 bv = make_float2(own1 ? Bs[c * RB * NZ + r1] : 0.f, own2 ? Bs[c * RB * NZ + r2] : 0.f);
-          const f2 d = p_sub(bv, y[c]);
-          if (OUT == OUT_RESID) {
-            if (own1) ob[c * st + c1] = pin1 ? 0.f : d.x;
-            if (own2) ob[c * st + c2] = pin2 ? 0.f : d.y;
+          bv[c] = make_float2(Bs[c * RB * NZ + r1], Bs[c * RB * NZ + r2]);
+          d[c] = p_sub(bv[c], y[c]);
+        }
+        if (OUT == OUT_RESID) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            if (own1) ob[c * st + c1] = pin1 ? 0.f : d[c].x;
+            if (own2) ob[c * st + c2] = pin2 ? 0.f : d[c].y;
+          }
+        } else {
+          const float* Is = S + oI;
+          f2 wd;
+          if (a.binv) {   // node-block sweep: d <- B d of both nodes
+            block_dir2(Is + 6 * r1, Is + 6 * r2, d);
+            wd = p_bc((float)a.omega);
           } else {
-            const f2 xv = a.binv ? p_fma(p_bc((float)a.omega), bd[c], u12[c]) : p_fma(wd, d, u12[c]);
+            wd = p_mul(p_bc((float)a.omega), make_float2(Is[r1], Is[r2]));
+          }
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const f2 xv = p_fma(wd, d[c], u12[c]);
             if (own1) ob[c * st + c1] = xv.x;
             if (own2) ob[c * st + c2] = xv.y;
             if (OUT == OUT_JACOBI_DOT) {
-              if (own1) acc += (double)xv.x * (double)bv.x;
-              if (own2) acc += (double)xv.y * (double)bv.y;
+              if (own1) acc += (double)xv.x * (double)bv[c].x;
+              if (own2) acc += (double)xv.y * (double)bv[c].y;
             }
           }
         }
