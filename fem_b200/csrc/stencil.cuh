@@ -623,11 +623,9 @@ __device__ __forceinline__ f2 p_bc(float s) { return make_float2(s, s); }
 // Node-block Jacobi direction of two nodes in the two lanes: d <- B d with
 // lane x the block at b1, lane y the block at b2 (layout of jacobi_dir).
 __device__ __forceinline__ void block_dir2(const float* __restrict__ b1, const float* __restrict__ b2, f2 (&d)[3]) {
-  const float2 p01 = *reinterpret_cast<const float2*>(b1), q01 = *reinterpret_cast<const float2*>(b2);
-  const float2 p23 = *reinterpret_cast<const float2*>(b1 + 2), q23 = *reinterpret_cast<const float2*>(b2 + 2);
-  const float2 p45 = *reinterpret_cast<const float2*>(b1 + 4), q45 = *reinterpret_cast<const float2*>(b2 + 4);
-  const f2 xx = make_float2(p01.x, q01.x), yy = make_float2(p01.y, q01.y), zz = make_float2(p23.x, q23.x);
-  const f2 xy = make_float2(p23.y, q23.y), xz = make_float2(p45.x, q45.x), yz = make_float2(p45.y, q45.y);
+  // one scalar load per lane and entry, straight into the pair's halves
+  const f2 xx = make_float2(b1[0], b2[0]), yy = make_float2(b1[1], b2[1]), zz = make_float2(b1[2], b2[2]);
+  const f2 xy = make_float2(b1[3], b2[3]), xz = make_float2(b1[4], b2[4]), yz = make_float2(b1[5], b2[5]);
   const f2 d0 = d[0], d1 = d[1], d2 = d[2];
   d[0] = p_fma(xz, d2, p_fma(xy, d1, p_mul(xx, d0)));
   d[1] = p_fma(yz, d2, p_fma(yy, d1, p_mul(xy, d0)));
