@@ -1329,6 +1329,9 @@ void autotune_level0_fp64(femh_handle* H) {
   std::vector<int> cands;
   for (int cand : {4, 8, 16, 32, 64, maxnx})
     if (cand <= maxnx && std::find(cands.begin(), cands.end(), cand) == cands.end()) cands.push_back(cand);
+  // large levels favour long chunks: scan from the longest, so the 25% rule
+  // stops before the slow short ones
+  if (L.ntot > (1 << 20)) std::reverse(cands.begin(), cands.end());
   std::vector<int> vars64 = {1, 2};
   if (L.bulk_ok64) vars64.push_back(6);
   if (H->cfg.stencil_variant == 6 && L.bulk_ok64) vars64 = {6};
@@ -1346,7 +1349,7 @@ void autotune_level0_fp64(femh_handle* H) {
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, H->ev0, H->ev1));
         ms_min = std::min(ms_min, ms);
-        if (rep >= 1 && ms_min > 2.0f) break;
+        if (ms_min > 8.0f || (rep >= 1 && ms_min > 2.0f)) break;   // one sample of a long launch suffices
       }
       if (verbose()) std::fprintf(stderr, "[femh] tune level 0 fp64 variant %d chunk %d: %.4f ms\n", var, cand, ms_min);
       if (ms_min < best_ms) {
@@ -1397,6 +1400,9 @@ void autotune_levels(femh_handle* H, bool mg) {
     std::vector<int> cands;
     for (int cand : {1, 2, 4, 8, 16, 32, 64, maxnx})
       if (cand <= maxnx && std::find(cands.begin(), cands.end(), cand) == cands.end()) cands.push_back(cand);
+    // large levels favour long chunks: scan from the longest (the 25% rule below
+    // then stops before the slow short ones); small levels from the shortest
+    if (L.ntot > (1 << 20)) std::reverse(cands.begin(), cands.end());
     const int reps = L.ntot < 65536 ? 7 : 3;   // small levels time in microseconds: more samples
     std::vector<int> vars = {1, 2};
     if (std::is_same<T, float>::value) vars = {2, 3, 4};
@@ -1406,9 +1412,9 @@ void autotune_levels(femh_handle* H, bool mg) {
     if (std::is_same<T, float>::value && L.bulk_ok && !L.grouped && L.cells.size() == 1) vars.push_back(7);
     if (std::is_same<T, double>::value && L.bulk_ok64) vars.push_back(6);
     if (H->cfg.stencil_variant > 0) vars = {H->cfg.stencil_variant};
-    // chunks in increasing order: a variant's scan stops once a chunk is 25% slower
-    // than its best so far (the time is unimodal in the chunk); launches of a few
-    // milliseconds are stable after two samples
+    // a variant's scan stops once a chunk is 25% slower than its best so far
+    // (the time is unimodal in the chunk); launches of a few
+    // milliseconds are stable after two samples, launches over 8 ms after one
     for (int var : vars) {
     float var_best = 1e30f;
     for (int cand : cands) {
@@ -1427,7 +1433,7 @@ void autotune_levels(femh_handle* H, bool mg) {
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, H->ev0, H->ev1));
         ms_min = std::min(ms_min, ms);
-        if (rep >= 1 && ms_min > 2.0f) break;
+        if (ms_min > 8.0f || (rep >= 1 && ms_min > 2.0f)) break;   // one sample of a long launch suffices
       }
       if (verbose()) std::fprintf(stderr, "[femh] tune level %zu variant %d chunk %d: %.4f ms\n", l, var, cand, ms_min);
       if (ms_min < best_ms) {
