@@ -1,6 +1,6 @@
 """GPU parity of the CUDA engine (through the C ABI) against the FP64 oracle.
 
-Bars (written here):
+Bars (the accuracy required of this path: C^H 1e-8 FP64 / 1e-6 mixed, gradients 1e-5):
   * operator apply, FP64:                 1e-13 relative (max-norm)
   * operator apply, FP32 kernels:         2e-6 relative (max-norm; FP32 rounding
                                           of rho-scaled coefficients, u and sums)
