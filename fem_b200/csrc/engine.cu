@@ -432,6 +432,11 @@ struct femh_handle {
   void* cg_q = nullptr;
   void* cg_rm = nullptr;        // FP32 copy of the FP64 residual (level-0 rhs of an FP32 V-cycle)
   CGState* d_state = nullptr;
+  BlockCG* d_bcg = nullptr;     // block PCG step matrices per cell
+  double* d_part_g = nullptr;   // block PCG 6x6 partials [2][sub-slots][36]
+  double* d_part_b = nullptr;   // block PCG ||r||^2 partials [sub-slots][6]
+  size_t part_g_slots = 0;      // slots of level 0 before any compaction (units keep their slot)
+  int bsub = 1;                 // block PCG: CTAs per level-0 node unit
   std::vector<CGState> state;
   double* d_part_s = nullptr;   // stencil partials [slots][6]
   double* d_part_n = nullptr;   // node partials [slots][6][2]
@@ -965,6 +970,14 @@ double* grad_target(femh_handle* H, double* user, int user_on_device) {
 // Extents of every multigrid level of one cell (x, y, z per level, finest
 // first): halve while every extent is even and >= 4 and the level has more
 // than coarse_max_nodes nodes.  Jacobi-PCG: the cell alone.
+// Block PCG over the load cases (config block_cg) applies to the multigrid
+// PCG with FP64 CG vectors; its search directions are kept in FP64 (FP32 or
+// BF16 directions lose the conjugacy of the block's weak directions: at 128^3
+// the block stalled for hundreds of iterations with FP32 directions).
+bool block_pcg(const femh_config& c) {
+  return c.block_cg && c.solver == FEMH_GMG_PCG && (c.precision == FEMH_FP64 || c.precision == FEMH_MIXED_PC);
+}
+
 std::vector<int> level_dims(const femh_config& c, int nx, int ny, int nz) {
   std::vector<int> d = {nx, ny, nz};
   if (c.solver != FEMH_GMG_PCG) return d;
@@ -986,7 +999,7 @@ double cell_setup_bytes(const femh_config& c, int nx, int ny, int nz) {
   const bool gmg = c.solver == FEMH_GMG_PCG;
   const bool mg32 = c.precision != FEMH_FP64;
   const double vsz = mixed ? 4 : 8, msz = mg32 ? 4 : 8, csz = mg32 ? 4 : 8;
-  const double psz = c.precision == FEMH_FP64 ? 8 : (c.store_bf16 ? 2 : 4);
+  const double psz = (c.precision == FEMH_FP64 || block_pcg(c)) ? 8 : (c.store_bf16 ? 2 : 4);
   const std::vector<int> d = level_dims(c, nx, ny, nz);
   const int nl = (int)d.size() / 3;
   double b = 0.0;
@@ -1037,7 +1050,7 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   H->nvox = off;
   const bool mg32 = c.precision != FEMH_FP64;   // multigrid hierarchy in FP32
   const size_t vsz = mixed ? sizeof(float) : sizeof(double);   // CG vectors
-  const size_t psz = c.precision == FEMH_FP64 ? sizeof(double)
+  const size_t psz = (c.precision == FEMH_FP64 || block_pcg(c)) ? sizeof(double)
                      : (c.store_bf16 ? sizeof(__nv_bfloat16) : sizeof(float));   // search directions
   const size_t msz = mg32 ? sizeof(float) : sizeof(double);
 
@@ -1186,6 +1199,12 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   const Level& L0 = H->levels[0];
   H->d_part_s = ar.arr<double>(std::max(L0.all.su.size(), L0.su64.size()) * kNumRhs);
   H->d_part_n = ar.arr<double>(L0.all.nu.size() * kNumRhs * 2);
+  H->part_g_slots = L0.all.nu.size();
+  H->bsub = 1;   // enough CTAs for two per SM in the block PCG's node kernels
+  while (H->bsub < 32 && (long long)H->part_g_slots * H->bsub < 2LL * std::max(H->nsm, 1)) H->bsub *= 2;
+  H->d_part_g = ar.arr<double>(H->part_g_slots * H->bsub * 72);
+  H->d_part_b = ar.arr<double>(H->part_g_slots * H->bsub * kNumRhs);
+  H->d_bcg = ar.arr<BlockCG>(nc);
   H->d_part_z = ar.arr<double>(std::max(L0.all.nu.size(), L0.all.su.size()) * kNumRhs);
   H->d_part_e = ar.arr<double>(L0.all.nu.size() * 22);   // 21 pair energies + sum of rho per slot
   H->d_C = ar.arr<double>(nc * 36);
@@ -1643,9 +1662,78 @@ struct Prec {
   using MC = TMC;
 };
 
+// Block PCG: directions dropped from G = P^T K P below this pivot ratio
+// (dependent to the accuracy of the preconditioned block: an FP32 V-cycle
+// resolves ~1e-4 in angle, an FP64 one ~1e-6 is still meaningful).
+template <typename TM> constexpr double block_drop() { return sizeof(TM) == 8 ? 1e-12 : 1e-8; }
+
+// Partials of a 6x6 product A^T B of each cell's block: the upper triangle
+// (SYM) or all 36 entries, per node slot, into `part`.
+template <bool SYM, typename TA, typename TB>
+void block_gram(femh_handle* H, const char* name, const TA* a, const TB* b, double* part) {
+  Level& L0 = H->levels[0];
+  const dim3 grid((unsigned)(L0.all.nu.size() * H->bsub));
+  Prof prof_(H, name, 18.0 * (sizeof(TA) + sizeof(TB)) * (double)L0.ntot);
+  k_bgram<SYM, TA, TB><<<grid, 256, 0, H->stream>>>(L0.d_cells, L0.all.d_nu, a, b, H->d_bcg, part, L0.ntot,
+                                                    H->bsub);
+  LAUNCH_CHECK(H);
+}
+
+// One block PCG iteration of the multigrid PCG (all live cells).
+template <class PR>
+void pcg_iteration_block(femh_handle* H, const typename PR::K* kcg) {
+  using TV = typename PR::V;
+  using TP = typename PR::P;
+  using TM = typename PR::M;
+  using TMC = typename PR::MC;
+  cudaStream_t s = H->stream;
+  Level& L0 = H->levels[0];
+  const int nc = H->ncells;
+  const int nsub = H->bsub;
+  const dim3 grid((unsigned)(L0.all.nu.size() * nsub));
+  TV* x = (TV*)H->cg_x;
+  TV* r = (TV*)H->cg_r;
+  TP* p = (TP*)H->cg_p;
+  TV* q = (TV*)H->cg_q;
+  TM* rm = (sizeof(TM) != sizeof(TV)) ? (TM*)H->cg_rm : nullptr;
+  CGState* stt = H->d_state;
+  double* part_a = H->d_part_g;                                        // [sub-slots][36]
+  double* part_b = H->d_part_g + H->part_g_slots * nsub * 36;          // [sub-slots][36]
+  stencil<TV, OUT_APPLY_DOT>(H, L0, false, (const TP*)p, q, (const TV*)nullptr, kcg, H->d_part_s, stt, 0.0);
+  block_gram<true, TP, TV>(H, "k_bgram_pq", (const TP*)p, (const TV*)q, part_a);
+  {
+    Prof prof_(H, "k_bfin_alpha", 0.0);
+    k_bfin_alpha<<<nc, 256, 0, s>>>(H->d_bcg, stt, L0.d_nu_sb, L0.d_nu_se, part_a, nc, block_drop<TM>(), nsub);
+    LAUNCH_CHECK(H);
+  }
+  {
+    Prof prof_(H, "k_bupdate",
+               18.0 * (5 * sizeof(TV) + sizeof(TP) + sizeof(TM) + (rm ? sizeof(TM) : 0)) * (double)L0.ntot +
+                   (L0.binv ? 24.0 : 4.0) * (double)L0.ntot);
+    k_bupdate<TV, TP, TV, TM><<<grid, 256, 0, s>>>(L0.d_cells, L0.all.d_nu, x, r, p, q, L0.invd, (TM*)L0.xa, rm,
+                                                   H->w_pre[0], H->d_bcg, H->d_part_b, L0.ntot, L0.binv, nsub);
+    LAUNCH_CHECK(H);
+  }
+  TM* z = rm ? vcycle<TM, TMC, TM>(H, rm, nullptr) : vcycle<TM, TMC, TV>(H, r, nullptr);
+  block_gram<false, TM, TV>(H, "k_bgram_zr", (const TM*)z, (const TV*)r, part_a);
+  block_gram<false, TV, TM>(H, "k_bgram_qz", (const TV*)q, (const TM*)z, part_b);
+  {
+    Prof prof_(H, "k_bfin_beta", 0.0);
+    k_bfin_beta<<<nc, 256, 0, s>>>(H->d_bcg, stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_b, part_a, part_b, nc,
+                                   block_drop<TM>(), nsub);
+    LAUNCH_CHECK(H);
+  }
+  {
+    Prof prof_(H, "k_bdir", 18.0 * (sizeof(TM) + 2 * sizeof(TP)) * (double)L0.ntot);
+    k_bdir<TP, TM><<<grid, 256, 0, s>>>(L0.d_cells, L0.all.d_nu, p, (const TM*)z, H->d_bcg, L0.ntot, 0, nsub);
+    LAUNCH_CHECK(H);
+  }
+}
+
 // One PCG iteration (all cells / load cases; inactive ones skip their work).
 template <class PR>
-void pcg_iteration(femh_handle* H, const typename PR::K* kcg) {
+void pcg_iteration(femh_handle* H, const typename PR::K* kcg, bool blk) {
+  if (blk) return pcg_iteration_block<PR>(H, kcg);
   using TV = typename PR::V;
   using TP = typename PR::P;
   using TM = typename PR::M;
@@ -1707,9 +1795,12 @@ void pcg_iteration(femh_handle* H, const typename PR::K* kcg) {
 // PCG on K x = scale*b for every (cell, rhs) whose state is active.
 // warm: x already holds the starting iterate and b is its residual; the
 // relative residual is measured against ||b_orig||^2 in H->d_nrm.
+// block: the GMG-PCG of the FP64 CG modes runs as block PCG over each cell's
+// load cases (config block_cg); a cell whose block fails is solved again one
+// load case at a time, from zero on the unreduced right-hand side H->b64.
 template <class PR, typename TB>
 void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, double tol, int iters_out[],
-         bool warm = false) {
+         bool warm = false, bool block = true) {
   using TV = typename PR::V;
   using TP = typename PR::P;
   using TM = typename PR::M;
@@ -1724,6 +1815,7 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
   TP* p = (TP*)H->cg_p;
   TM* rm = (gmg && sizeof(TM) != sizeof(TV)) ? (TM*)H->cg_rm : nullptr;
   CGState* stt = H->d_state;
+  const bool blk = block && block_pcg(c) && sizeof(TV) == 8 && sizeof(TP) == 8;
   for (auto& S : H->state) {
     S.tol = tol;
     S.max_iter = max_iter;
@@ -1749,6 +1841,28 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
                                                           L0.invd, H->w_pre[0], stt, L0.ntot, L0.binv);
       LAUNCH_CHECK(H);
     }
+    if (blk) {   // block PCG: Z^T R of the start, P = Z
+      {
+        Prof prof_(H, "k_binit", 0.0);
+        k_binit<<<cdiv(nc, 128), 128, 0, s>>>(H->d_bcg, stt, nc);
+        LAUNCH_CHECK(H);
+      }
+      TM* z = rm ? vcycle<TM, TMC, TM>(H, rm, nullptr) : vcycle<TM, TMC, TV>(H, r, nullptr);
+      block_gram<false, TM, TV>(H, "k_bgram_zr", (const TM*)z, (const TV*)r, H->d_part_g);
+      {
+        Prof prof_(H, "k_bfin_rz", 0.0);
+        k_bfin_rz<<<nc, 256, 0, s>>>(H->d_bcg, stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_g, nc, H->bsub);
+        LAUNCH_CHECK(H);
+      }
+      {
+        Prof prof_(H, "k_bdir", 0.0);
+        k_bdir<TP, TM><<<dim3((unsigned)(L0.all.nu.size() * H->bsub)), 256, 0, s>>>(
+            L0.d_cells, L0.all.d_nu, p, (const TM*)z, H->d_bcg, L0.ntot, 1, H->bsub);
+        LAUNCH_CHECK(H);
+      }
+    }
+  }
+  if (gmg && !blk) {
     const bool fuse = fuse_rz(H);
     double* dp = fuse ? H->d_part_z : nullptr;
     TM* z = rm ? vcycle<TM, TMC, TM>(H, rm, dp) : vcycle<TM, TMC, TV>(H, r, dp);
@@ -1804,7 +1918,7 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
     H->cap_count = 0;
     CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     try {
-      for (int i = 0; i < chunk; ++i) pcg_iteration<PR>(H, kcg);
+      for (int i = 0; i < chunk; ++i) pcg_iteration<PR>(H, kcg, blk);
       k_while_cond<<<1, 1024, 0, s>>>(cond, H->d_state, nc, listed, H->d_loop, chunk, limit);
       LAUNCH_CHECK(H);
     } catch (...) {
@@ -1847,7 +1961,7 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
         H->launches += graph_kernels * (long long)std::max(1, (loop_now - done) / chunk);
         done = loop_now;
       } else {
-        for (int i = 0; i < chunk; ++i) pcg_iteration<PR>(H, kcg);
+        for (int i = 0; i < chunk; ++i) pcg_iteration<PR>(H, kcg, blk);
         done += chunk;
         CK(cudaMemcpyAsync(H->state.data(), stt, sizeof(CGState) * H->state.size(), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
@@ -1888,6 +2002,18 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
   if (exec) CK(cudaGraphExecDestroy(exec));
   restore();
   for (int t = 0; t < nc * kNumRhs; ++t) iters_out[t] += H->state[t].iters;
+  if (blk) {   // cells whose block step matrices turned indefinite: one load case at a time
+    bool again = false;
+    for (auto& S : H->state) {
+      if (S.status != CG_BLOCK_FAIL) continue;
+      const double sc = S.scale;
+      S = CGState{};
+      S.active = 1;
+      S.scale = sc;
+      again = true;
+    }
+    if (again) pcg<PR>(H, (const TB*)H->b64, kcg, max_iter, tol, iters_out, false, false);
+  }
 }
 
 // FP64 true residual r64 = b64 - K x64 and its norm per (cell, rhs) -> host.
@@ -1980,6 +2106,8 @@ void solve_all(femh_handle* H, std::vector<femh_solve_info>& infos) {
     }
     if (c.precision == FEMH_FP64)
       pcg<Prec<double, double, double, double, double>>(H, b0, H->kc64, c.max_iter, c.tol, iters.data(), warm);
+    else if (block_pcg(c))   // block PCG: FP64 search directions
+      pcg<Prec<double, double, double, float, float>>(H, b0, H->kc64, c.max_iter, c.tol, iters.data(), warm);
     else if (c.store_bf16)   // FP64 CG and operator, FP32 multigrid, bf16 search directions
       pcg<Prec<double, __nv_bfloat16, double, float, float>>(H, b0, H->kc64, c.max_iter, c.tol, iters.data(), warm);
     else   // FP64 CG and operator, FP32 multigrid preconditioner and search directions
@@ -2174,6 +2302,7 @@ void check_config(const femh_config& c) {
   if (c.stencil_variant < 0 || c.stencil_variant > 7) throw FemhError{FEMH_E_ARG, "stencil_variant must be 0..7"};
   if (!(c.cheb_ratio == 0.0 || c.cheb_ratio > 1.0)) throw FemhError{FEMH_E_ARG, "cheb_ratio must be 0 or > 1"};
   if (c.block_jacobi != 0 && c.block_jacobi != 1) throw FemhError{FEMH_E_ARG, "block_jacobi must be 0 or 1"};
+  if (c.block_cg != 0 && c.block_cg != 1) throw FemhError{FEMH_E_ARG, "block_cg must be 0 or 1"};
   if (c.coarse_avg < 0 || c.coarse_avg > 2) throw FemhError{FEMH_E_ARG, "coarse_avg must be 0, 1 or 2"};
   if (!(c.E_s > 0.0) || c.E_min < 0.0 || !(c.rho_max >= c.rho_min))
     throw FemhError{FEMH_E_ARG, "bad material law parameters"};
@@ -2213,6 +2342,7 @@ femh_status femh_config_default(femh_config* c) {
   c->warm_start = 0;
   c->cheb_ratio = 64.0;   // 128^3 smooth cell, mixed: 146 iterations (2+2, omega) -> 86
   c->block_jacobi = 1;   // 128^3 smooth cell, mixed: 87 iterations -> 75, 219 -> 204 ms
+  c->block_cg = 1;
   return FEMH_OK;
 }
 

@@ -74,7 +74,9 @@ struct CGState {
 // halved for this many iterations: it has reached what its arithmetic resolves,
 // and the next outer step (FP64 residual) continues from there.
 constexpr int kInnerStallWindow = 200;
-enum CGStatus : int { CG_RUNNING = 0, CG_CONVERGED = 1, CG_MAXITER = 2, CG_BREAKDOWN = 3 };
+// CG_BLOCK_FAIL: a block PCG step matrix turned indefinite; the cell's load
+// cases are solved again one at a time.
+enum CGStatus : int { CG_RUNNING = 0, CG_CONVERGED = 1, CG_MAXITER = 2, CG_BREAKDOWN = 3, CG_BLOCK_FAIL = 4 };
 
 template <typename T> struct VT { using type = T; };
 

@@ -323,6 +323,408 @@ __device__ __forceinline__ double sum_slots(const double* part, int b, int e, in
   return s;
 }
 
+// ------------------------------------------------------ block PCG ---
+// Block conjugate gradients over the six load cases of a cell (O'Leary,
+// Linear Algebra Appl. 29, 1980): they share the operator and the
+// preconditioner, so one Krylov space serves all six and the scalar steps
+// become 6x6 matrices.  Each new search block is made K-conjugate to the
+// previous one explicitly (the flexible form, as in Notay's flexible CG,
+// SIAM J. Sci. Comput. 22, 2000), so an FP32 V-cycle that is symmetric only to
+// its rounding keeps the directions conjugate:
+//   G = P^T K P,  alpha = G^+ (Z^T R),  X += P alpha,  R -= (K P) alpha,
+//   Z = M R,      beta = -G^+ ((K P)^T Z),  P = Z + P beta.
+// G^+ solves by Cholesky and drops a direction whose pivot falls below `drop`
+// of its diagonal (dependent on the earlier ones to the accuracy of the
+// preconditioned block: 1e-12 with an FP64 V-cycle, 1e-8 with an FP32 one).
+// Load cases that are not live at the start (a zero right-hand side) stay out
+// of every product.
+struct BlockCG {
+  double g[36];       // P^T K P of the current search block, symmetric, row-major
+  double zr[36];      // zr[k * 6 + j] = z_k . r_j
+  double alpha[36];   // alpha[i * 6 + j]: weight of direction i in load case j
+  double beta[36];    // beta[i * 6 + j]: weight of old direction i in new direction j
+  double best;        // smallest worst-case relative residual of the block so far
+  int since;          // iterations since that last halved
+  int mask;           // load cases in the block (bit j)
+  int live;           // 1 while the block iterates
+};
+// A block whose worst relative residual has not halved for this many
+// iterations has stalled: its cell is solved again one load case at a time.
+constexpr int kBlockStallWindow = 200;
+
+// Index of (i, j), i <= j, in the 21 upper-triangle entries of a 6x6 matrix.
+__host__ __device__ constexpr int sym6(int i, int j) { return i * 6 - i * (i - 1) / 2 + (j - i); }
+
+// G X = s B (6x6, row-major) by Cholesky on the columns in mask, a column
+// with a pivot below drop times its diagonal dropped (its row of X is 0).
+// Returns false if a pivot is below -1e-8 times its diagonal (G indefinite
+// beyond rounding), not finite, or no column is kept.
+__device__ __noinline__ bool chol_solve6(const double* __restrict__ G, const double* __restrict__ B, double sgn,
+                                         double* __restrict__ X, int mask, double drop) {
+  double L[6][6];
+  int keep = 0;
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const double gkk = G[k * 6 + k];
+    double d = gkk;
+#pragma unroll
+    for (int j = 0; j < k; ++j)
+      if (keep >> j & 1) d -= L[k][j] * L[k][j];
+    const bool in = mask >> k & 1;
+    if (in && (!isfinite(d) || d < -1e-8 * fabs(gkk))) ok = false;
+    const bool use = in && gkk > 0.0 && d > drop * gkk;
+    const double lkk = use ? sqrt(d) : 1.0;
+    L[k][k] = lkk;
+#pragma unroll
+    for (int i = k + 1; i < 6; ++i) {
+      double v = G[i * 6 + k];
+#pragma unroll
+      for (int j = 0; j < k; ++j)
+        if (keep >> j & 1) v -= L[i][j] * L[k][j];
+      L[i][k] = use ? v / lkk : 0.0;
+    }
+    if (use) keep |= 1 << k;
+  }
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    double y[6], x[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      double v = sgn * B[k * 6 + c];
+#pragma unroll
+      for (int j = 0; j < k; ++j)
+        if (keep >> j & 1) v -= L[k][j] * y[j];
+      y[k] = (keep >> k & 1) ? v / L[k][k] : 0.0;
+    }
+#pragma unroll
+    for (int k = 5; k >= 0; --k) {
+      double v = y[k];
+#pragma unroll
+      for (int j = k + 1; j < 6; ++j)
+        if (keep >> j & 1) v -= L[j][k] * x[j];
+      x[k] = (keep >> k & 1) ? v / L[k][k] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) X[k * 6 + c] = x[k];
+  }
+  return ok && keep != 0;
+}
+
+// The block kernels split each node unit into S sub-ranges, one CTA each (S
+// > 1 gives small cells enough CTAs); partial sums go to sub-slot slot*S + s.
+struct SubUnit {
+  NodeUnit u;
+  long long begin, end;
+  long long sub;   // partial-sum index
+};
+__device__ __forceinline__ SubUnit sub_unit(const NodeUnit* units, int S) {
+  const int s = (int)(blockIdx.x % (unsigned)S);
+  SubUnit r;
+  r.u = units[blockIdx.x / (unsigned)S];
+  const long long len = r.u.end - r.u.begin;
+  r.begin = r.u.begin + len * s / S;
+  r.end = r.u.begin + len * (s + 1) / S;
+  r.sub = (long long)r.u.slot * S + s;
+  return r;
+}
+
+// Partials of the 6x6 matrix A^T B of one cell's block per sub-slot: its
+// upper triangle (SYM, 21 values) or all 36 entries a_i . b_j (i * 6 + j);
+// columns outside the block's mask read as 0.
+template <bool SYM, typename TA, typename TB>
+__global__ void __launch_bounds__(256, 2)
+k_bgram(const CellDesc* cells, const NodeUnit* units, const TA* __restrict__ a, const TB* __restrict__ b,
+        const BlockCG* bst, double* __restrict__ part, long long ntot, int nsub) {
+  constexpr int NV = SYM ? 21 : 36;
+  const SubUnit su = sub_unit(units, nsub);
+  const CellDesc cd = cells[su.u.cell];
+  const int mask = bst[cd.id].live ? bst[cd.id].mask : 0;
+  double v[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = 0.0;
+  if (mask) {
+    for (long long n = su.begin + threadIdx.x; n < su.end; n += blockDim.x) {
+      const long long g = cd.off + n;
+#pragma unroll 1
+      for (int c = 0; c < 3; ++c) {
+        double av[6], bv[6];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+          const long long o = ((long long)j * 3 + c) * ntot + g;
+          const bool in = mask >> j & 1;
+          av[j] = in ? (double)ld_val(a + o) : 0.0;
+          bv[j] = in ? (double)ld_val(b + o) : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+          for (int j = SYM ? i : 0; j < 6; ++j) v[SYM ? sym6(i, j) : i * 6 + j] += av[i] * bv[j];
+      }
+    }
+  }
+  __shared__ double red[32 * NV];
+  block_reduce<NV>(v, red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) part[su.sub * NV + k] = v[k];
+}
+
+// Sum of a cell's per-slot partials over its slot range [b, e) by a
+// 256-thread CTA in a fixed order (deterministic): thread t adds value
+// t % NV of the slots b + t / NV, b + t / NV + G, ... (G = 256 / NV groups,
+// coalesced rows), then thread k < NV adds the G group sums of value k.
+// out[k] (shared memory) is valid after the call in every thread.
+template <int NV>
+__device__ __forceinline__ void cta_sum_slots(const double* __restrict__ part, int b, int e, double* red,
+                                              double* out) {
+  constexpr int G = 256 / NV;
+  const int t = threadIdx.x, k = t % NV, grp = t / NV;
+  if (grp < G) {
+    double acc = 0.0;
+    for (int sl = b + grp; sl < e; sl += G) acc += part[(long long)sl * NV + k];
+    red[grp * NV + k] = acc;
+  }
+  __syncthreads();
+  if (t < NV) {
+    double acc = 0.0;
+    for (int g2 = 0; g2 < G; ++g2) acc += red[g2 * NV + t];
+    out[t] = acc;
+  }
+  __syncthreads();
+}
+
+// Full 6x6 matrix from 21 upper-triangle values (sym) or 36 row-major ones.
+__device__ __forceinline__ void expand6(const double* v, bool sym, double* M) {
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) M[i * 6 + j] = sym ? v[i <= j ? sym6(i, j) : sym6(j, i)] : v[i * 6 + j];
+}
+
+// The block stops: its load cases leave the loop with `status`.
+__device__ void block_stop(BlockCG& B, CGState* stt, int cell, int status) {
+  B.live = 0;
+#pragma unroll 1
+  for (int j = 0; j < kNumRhs; ++j)
+    if (B.mask >> j & 1) {
+      CGState& S = stt[cell * kNumRhs + j];
+      S.active = 0;
+      S.status = status == CG_MAXITER && S.rel < S.tol ? CG_CONVERGED : status;
+    }
+}
+
+// z_j . r_j of every load case of the block positive: the preconditioner is
+// positive on the current residuals.
+__device__ __forceinline__ bool zr_positive(const double* Z, int mask) {
+  bool ok = true;
+#pragma unroll
+  for (int j = 0; j < 6; ++j)
+    if (mask >> j & 1) ok = ok && Z[j * 7] > 0.0 && isfinite(Z[j * 7]);
+  return ok;
+}
+
+// After k_fin_init: the block of each cell is its live load cases.
+__global__ void k_binit(BlockCG* bst, const CGState* stt, int ncells) {
+  const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= ncells) return;
+  int mask = 0;
+  for (int j = 0; j < kNumRhs; ++j)
+    if (stt[cell * kNumRhs + j].active) mask |= 1 << j;
+  BlockCG& B = bst[cell];
+  B.mask = mask;
+  B.live = mask != 0;
+  B.best = INFINITY;
+  B.since = 0;
+  for (int k = 0; k < 36; ++k) B.alpha[k] = B.beta[k] = 0.0;
+}
+
+// After the first preconditioner application: Z^T R of the start (beta = 0).
+// One 256-thread CTA per cell.
+__global__ void __launch_bounds__(256) k_bfin_rz(BlockCG* bst, CGState* stt, const int* sb, const int* se,
+                                                 const double* part_zr, int ncells, int nsub) {
+  const int cell = blockIdx.x;
+  BlockCG& B = bst[cell];
+  if (!B.live) return;
+  __shared__ double red[256], Z[36];
+  cta_sum_slots<36>(part_zr, sb[cell] * nsub, se[cell] * nsub, red, Z);
+  if (threadIdx.x != 0) return;
+  if (!zr_positive(Z, B.mask)) return block_stop(B, stt, cell, CG_BLOCK_FAIL);
+  for (int k = 0; k < 36; ++k) B.zr[k] = Z[k];
+}
+
+// G = P^T K P, alpha = G^+ Z^T R.  One 256-thread CTA per cell.
+__global__ void __launch_bounds__(256) k_bfin_alpha(BlockCG* bst, CGState* stt, const int* sb, const int* se,
+                                                    const double* part_g, int ncells, double drop, int nsub) {
+  const int cell = blockIdx.x;
+  BlockCG& B = bst[cell];
+  if (!B.live) return;
+  __shared__ double red[256], g[21], G[36], A[36], ZR[36];
+  cta_sum_slots<21>(part_g, sb[cell] * nsub, se[cell] * nsub, red, g);
+  if (threadIdx.x < 36) ZR[threadIdx.x] = B.zr[threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  expand6(g, true, G);
+  if (!chol_solve6(G, ZR, 1.0, A, B.mask, drop)) return block_stop(B, stt, cell, CG_BLOCK_FAIL);
+  for (int k = 0; k < 36; ++k) {
+    B.alpha[k] = A[k];
+    B.g[k] = G[k];
+  }
+}
+
+// After the update and the preconditioner: convergence of every load case of
+// the block, then beta = -G^+ (K P)^T Z.  One 256-thread CTA per cell.
+__global__ void __launch_bounds__(256) k_bfin_beta(BlockCG* bst, CGState* stt, const int* sb, const int* se,
+                                                   const double* part_upd, const double* part_zr,
+                                                   const double* part_qz, int ncells, double drop, int nsub) {
+  const int cell = blockIdx.x;
+  BlockCG& B = bst[cell];
+  if (!B.live) return;
+  const int b = sb[cell] * nsub, e = se[cell] * nsub;
+  __shared__ double red[256], Z[36], Q[36], T[36], G[36], rr[kNumRhs];
+  cta_sum_slots<36>(part_zr, b, e, red, Z);
+  cta_sum_slots<36>(part_qz, b, e, red, Q);
+  cta_sum_slots<kNumRhs>(part_upd, b, e, red, rr);
+  if (threadIdx.x < 36) G[threadIdx.x] = B.g[threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  bool all = true, spent = false, bad = false;
+  double worst = 0.0;
+  for (int j = 0; j < kNumRhs; ++j) {
+    if (!(B.mask >> j & 1)) continue;
+    CGState& S = stt[cell * kNumRhs + j];
+    S.rr = rr[j];
+    S.iters += 1;
+    S.rel = sqrt(S.rr / S.bnorm2);
+    all = all && S.rel < S.tol;
+    spent = spent || S.iters >= S.max_iter;
+    bad = bad || !isfinite(S.rel);
+    worst = fmax(worst, S.rel);
+  }
+  if (all) return block_stop(B, stt, cell, CG_CONVERGED);
+  if (bad) return block_stop(B, stt, cell, CG_BREAKDOWN);
+  if (spent) return block_stop(B, stt, cell, CG_MAXITER);
+  if (worst < 0.5 * B.best) {
+    B.best = worst;
+    B.since = 0;
+  } else if (++B.since >= kBlockStallWindow) {
+    return block_stop(B, stt, cell, CG_BLOCK_FAIL);
+  }
+  if (!zr_positive(Z, B.mask) || !chol_solve6(G, Q, -1.0, T, B.mask, drop))
+    return block_stop(B, stt, cell, CG_BLOCK_FAIL);
+  for (int k = 0; k < 36; ++k) {
+    B.beta[k] = T[k];
+    B.zr[k] = Z[k];
+  }
+}
+
+// X += P alpha, R -= Q alpha (Q = K P) for the load cases of each live block,
+// with ||r||^2 partials per load case ([sub-slot][6]) and, for the multigrid, the first
+// smoothing sweep z0 = omega D^-1 r and the residual copy rm of the V-cycle.
+// 256 threads; a node's new residuals wait in shared memory for the 3x3
+// node-block sweep (registers kept for three CTAs per SM).
+template <typename TV, typename TP, typename TQ, typename TZ>
+__global__ void __launch_bounds__(256, 3)
+k_bupdate(const CellDesc* cells, const NodeUnit* units, TV* __restrict__ x, TV* __restrict__ r,
+          const TP* __restrict__ p, const TQ* __restrict__ q, const float* __restrict__ invd, TZ* __restrict__ z0,
+          TZ* __restrict__ rm, double omega, const BlockCG* bst, double* __restrict__ part, long long ntot,
+          const float* __restrict__ binv, int nsub) {
+  const SubUnit su = sub_unit(units, nsub);
+  const CellDesc cd = cells[su.u.cell];
+  const int mask = bst[cd.id].live ? bst[cd.id].mask : 0;
+  __shared__ double al[36];
+  __shared__ double rs[kNumRhs * 3][256];
+  if (threadIdx.x < 36) al[threadIdx.x] = bst[cd.id].alpha[threadIdx.x];
+  __syncthreads();
+  double v[kNumRhs];
+#pragma unroll
+  for (int j = 0; j < kNumRhs; ++j) v[j] = 0.0;
+  if (mask) {
+    for (long long n = su.begin + threadIdx.x; n < su.end; n += blockDim.x) {
+      const long long g = cd.off + n;
+#pragma unroll 1
+      for (int c = 0; c < 3; ++c) {
+        double pv[kNumRhs], qv[kNumRhs];
+#pragma unroll
+        for (int i = 0; i < kNumRhs; ++i) {
+          const long long o = ((long long)i * 3 + c) * ntot + g;
+          const bool in = mask >> i & 1;
+          pv[i] = in ? (double)ld_val(p + o) : 0.0;
+          qv[i] = in ? (double)ld_val(q + o) : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < kNumRhs; ++j) {
+          if (!(mask >> j & 1)) continue;
+          double dx = 0.0, dr = 0.0;
+#pragma unroll
+          for (int i = 0; i < kNumRhs; ++i) {
+            dx += al[i * 6 + j] * pv[i];
+            dr += al[i * 6 + j] * qv[i];
+          }
+          const long long o = ((long long)j * 3 + c) * ntot + g;
+          const double rj = (n == 0) ? 0.0 : (double)ld_val(r + o) - dr;
+          st_val(x + o, (double)ld_val(x + o) + dx);
+          st_val(r + o, rj);
+          if (rm) st_val(rm + o, rj);
+          v[j] += rj * rj;
+          rs[j * 3 + c][threadIdx.x] = rj;
+        }
+      }
+      if (z0) {
+        const double id = binv ? 0.0 : (double)invd[g];
+#pragma unroll 1
+        for (int j = 0; j < kNumRhs; ++j) {
+          if (!(mask >> j & 1)) continue;
+          double d[3] = {rs[j * 3][threadIdx.x], rs[j * 3 + 1][threadIdx.x], rs[j * 3 + 2][threadIdx.x]};
+          jacobi_dir<double>(binv, g, id, d);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) st_val(z0 + ((long long)j * 3 + c) * ntot + g, omega * d[c]);
+        }
+      }
+    }
+  }
+  __shared__ double red[32 * kNumRhs];
+  block_reduce<kNumRhs>(v, red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int j = 0; j < kNumRhs; ++j) part[su.sub * kNumRhs + j] = v[j];
+}
+
+// P = Z + P beta for the load cases of each live block (first: P = Z).
+template <typename TP, typename TZ>
+__global__ void __launch_bounds__(256, 3)
+k_bdir(const CellDesc* cells, const NodeUnit* units, TP* __restrict__ p, const TZ* __restrict__ z,
+       const BlockCG* bst, long long ntot, int first, int nsub) {
+  const SubUnit su = sub_unit(units, nsub);
+  const CellDesc cd = cells[su.u.cell];
+  const int mask = bst[cd.id].live ? bst[cd.id].mask : 0;
+  __shared__ double be[36];
+  if (threadIdx.x < 36) be[threadIdx.x] = first ? 0.0 : bst[cd.id].beta[threadIdx.x];
+  __syncthreads();
+  if (!mask) return;
+  const bool rd = !first;
+  for (long long n = su.begin + threadIdx.x; n < su.end; n += blockDim.x) {
+    const long long g = cd.off + n;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double pv[kNumRhs], zv[kNumRhs];
+#pragma unroll
+      for (int i = 0; i < kNumRhs; ++i) {
+        const long long o = ((long long)i * 3 + c) * ntot + g;
+        const bool in = mask >> i & 1;
+        pv[i] = (rd && in) ? (double)ld_val(p + o) : 0.0;
+        zv[i] = in ? (double)ld_val(z + o) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < kNumRhs; ++j) {
+        if (!(mask >> j & 1)) continue;
+        double pj = zv[j];
+#pragma unroll
+        for (int i = 0; i < kNumRhs; ++i) pj += be[i * 6 + j] * pv[i];
+        st_val(p + ((long long)j * 3 + c) * ntot + g, pj);
+      }
+    }
+  }
+}
+
 // One warp per (cell, rhs) in the finalisation kernels.
 #define FIN_PROLOGUE                                                         \
   const int t = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5); \

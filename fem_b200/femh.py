@@ -55,7 +55,7 @@ class _Config(ctypes.Structure):
         ("inner_tol", ctypes.c_double), ("max_outer", ctypes.c_int),
         ("store_bf16", ctypes.c_int), ("graph_chunk", ctypes.c_int), ("coarse_avg", ctypes.c_int),
         ("autotune", ctypes.c_int), ("stencil_variant", ctypes.c_int), ("warm_start", ctypes.c_int),
-        ("cheb_ratio", ctypes.c_double), ("block_jacobi", ctypes.c_int),
+        ("cheb_ratio", ctypes.c_double), ("block_jacobi", ctypes.c_int), ("block_cg", ctypes.c_int),
     ]
 
 
@@ -143,6 +143,7 @@ class Config:
     warm_start: int = 0
     cheb_ratio: float = 64.0
     block_jacobi: int = 1
+    block_cg: int = 1
 
     def to_c(self) -> _Config:
         c = _Config()

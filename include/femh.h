@@ -111,6 +111,11 @@ typedef struct {
                              Jacobi, D = the 3x3 diagonal blocks of K (the three
                              displacement components of a node solved together; they
                              couple where the coefficients jump) */
+  int block_cg;           /* GMG-PCG with FP64 CG (FEMH_FP64, FEMH_MIXED_PC), cold start:
+                             1 block conjugate gradients over the six load cases of a cell
+                             (one Krylov space, 6x6 step matrices; a cell whose block turns
+                             indefinite is solved again case by case), 0 six independent
+                             PCG runs */
 } femh_config;
 
 typedef struct {
