@@ -436,7 +436,8 @@ struct femh_handle {
   double* d_part_g = nullptr;   // block PCG 6x6 partials [2][sub-slots][36]
   double* d_part_b = nullptr;   // block PCG ||r||^2 partials [sub-slots][6]
   size_t part_g_slots = 0;      // slots of level 0 before any compaction (units keep their slot)
-  int bsub = 1;                 // block PCG: CTAs per level-0 node unit
+  int bsub = 1;                 // block PCG update / direction: CTAs per level-0 node unit
+  int bsub_g = 1;               // block PCG Gram kernels: CTAs per level-0 node unit
   std::vector<CGState> state;
   double* d_part_s = nullptr;   // stencil partials [slots][6]
   double* d_part_n = nullptr;   // node partials [slots][6][2]
@@ -1200,9 +1201,17 @@ void build_setup(femh_handle* H, const std::vector<int>& shapes, const std::vect
   H->d_part_s = ar.arr<double>(std::max(L0.all.su.size(), L0.su64.size()) * kNumRhs);
   H->d_part_n = ar.arr<double>(L0.all.nu.size() * kNumRhs * 2);
   H->part_g_slots = L0.all.nu.size();
-  H->bsub = 1;   // enough CTAs for two per SM in the block PCG's node kernels
-  while (H->bsub < 32 && (long long)H->part_g_slots * H->bsub < 2LL * std::max(H->nsm, 1)) H->bsub *= 2;
-  H->d_part_g = ar.arr<double>(H->part_g_slots * H->bsub * 72);
+  // CTAs per level-0 node unit in the block PCG's kernels.  The update and
+  // direction kernels (three 256-thread CTAs per SM) get >= 16 CTAs per SM, so
+  // the last wave is a small part of the launch (128^3: 1024 units -> 4096
+  // CTAs; ncu showed 1024 CTAs in 2.3 waves at 23-33% of the SMs' warps);
+  // the Gram kernels only enough for two per SM, because every extra CTA adds
+  // 21-36 partial sums that the per-cell finalisation reads back.
+  const long long nsm = std::max(H->nsm, 1);
+  H->bsub = H->bsub_g = 1;
+  while (H->bsub < 32 && (long long)H->part_g_slots * H->bsub < 16 * nsm) H->bsub *= 2;
+  while (H->bsub_g < 32 && (long long)H->part_g_slots * H->bsub_g < 2 * nsm) H->bsub_g *= 2;
+  H->d_part_g = ar.arr<double>(H->part_g_slots * H->bsub_g * 72);
   H->d_part_b = ar.arr<double>(H->part_g_slots * H->bsub * kNumRhs);
   H->d_bcg = ar.arr<BlockCG>(nc);
   H->d_part_z = ar.arr<double>(std::max(L0.all.nu.size(), L0.all.su.size()) * kNumRhs);
@@ -1672,10 +1681,10 @@ template <typename TM> constexpr double block_drop() { return sizeof(TM) == 8 ? 
 template <bool SYM, typename TA, typename TB>
 void block_gram(femh_handle* H, const char* name, const TA* a, const TB* b, double* part) {
   Level& L0 = H->levels[0];
-  const dim3 grid((unsigned)(L0.all.nu.size() * H->bsub));
+  const dim3 grid((unsigned)(L0.all.nu.size() * H->bsub_g));
   Prof prof_(H, name, 18.0 * (sizeof(TA) + sizeof(TB)) * (double)L0.ntot);
   k_bgram<SYM, TA, TB><<<grid, 256, 0, H->stream>>>(L0.d_cells, L0.all.d_nu, a, b, H->d_bcg, part, L0.ntot,
-                                                    H->bsub);
+                                                    H->bsub_g);
   LAUNCH_CHECK(H);
 }
 
@@ -1697,13 +1706,14 @@ void pcg_iteration_block(femh_handle* H, const typename PR::K* kcg) {
   TV* q = (TV*)H->cg_q;
   TM* rm = (sizeof(TM) != sizeof(TV)) ? (TM*)H->cg_rm : nullptr;
   CGState* stt = H->d_state;
-  double* part_a = H->d_part_g;                                        // [sub-slots][36]
-  double* part_b = H->d_part_g + H->part_g_slots * nsub * 36;          // [sub-slots][36]
+  const int nsub_g = H->bsub_g;
+  double* part_a = H->d_part_g;                                        // [Gram sub-slots][36]
+  double* part_b = H->d_part_g + H->part_g_slots * nsub_g * 36;        // [Gram sub-slots][36]
   stencil<TV, OUT_APPLY_DOT>(H, L0, false, (const TP*)p, q, (const TV*)nullptr, kcg, H->d_part_s, stt, 0.0);
   block_gram<true, TP, TV>(H, "k_bgram_pq", (const TP*)p, (const TV*)q, part_a);
   {
     Prof prof_(H, "k_bfin_alpha", 0.0);
-    k_bfin_alpha<<<nc, 256, 0, s>>>(H->d_bcg, stt, L0.d_nu_sb, L0.d_nu_se, part_a, nc, block_drop<TM>(), nsub);
+    k_bfin_alpha<<<nc, 256, 0, s>>>(H->d_bcg, stt, L0.d_nu_sb, L0.d_nu_se, part_a, nc, block_drop<TM>(), nsub_g);
     LAUNCH_CHECK(H);
   }
   {
@@ -1720,7 +1730,7 @@ void pcg_iteration_block(femh_handle* H, const typename PR::K* kcg) {
   {
     Prof prof_(H, "k_bfin_beta", 0.0);
     k_bfin_beta<<<nc, 256, 0, s>>>(H->d_bcg, stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_b, part_a, part_b, nc,
-                                   block_drop<TM>(), nsub);
+                                   block_drop<TM>(), nsub_g, nsub);
     LAUNCH_CHECK(H);
   }
   {
@@ -1851,7 +1861,7 @@ void pcg(femh_handle* H, const TB* b, const typename PR::K* kcg, int max_iter, d
       block_gram<false, TM, TV>(H, "k_bgram_zr", (const TM*)z, (const TV*)r, H->d_part_g);
       {
         Prof prof_(H, "k_bfin_rz", 0.0);
-        k_bfin_rz<<<nc, 256, 0, s>>>(H->d_bcg, stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_g, nc, H->bsub);
+        k_bfin_rz<<<nc, 256, 0, s>>>(H->d_bcg, stt, L0.d_nu_sb, L0.d_nu_se, H->d_part_g, nc, H->bsub_g);
         LAUNCH_CHECK(H);
       }
       {

@@ -571,18 +571,20 @@ __global__ void __launch_bounds__(256) k_bfin_alpha(BlockCG* bst, CGState* stt, 
 }
 
 // After the update and the preconditioner: convergence of every load case of
-// the block, then beta = -G^+ (K P)^T Z.  One 256-thread CTA per cell.
+// the block, then beta = -G^+ (K P)^T Z.  One 256-thread CTA per cell; the
+// Gram partials come in nsub_g sub-slots per slot, the ||r||^2 ones in nsub.
 __global__ void __launch_bounds__(256) k_bfin_beta(BlockCG* bst, CGState* stt, const int* sb, const int* se,
                                                    const double* part_upd, const double* part_zr,
-                                                   const double* part_qz, int ncells, double drop, int nsub) {
+                                                   const double* part_qz, int ncells, double drop, int nsub_g,
+                                                   int nsub) {
   const int cell = blockIdx.x;
   BlockCG& B = bst[cell];
   if (!B.live) return;
-  const int b = sb[cell] * nsub, e = se[cell] * nsub;
+  const int b = sb[cell] * nsub_g, e = se[cell] * nsub_g;
   __shared__ double red[256], Z[36], Q[36], T[36], G[36], rr[kNumRhs];
   cta_sum_slots<36>(part_zr, b, e, red, Z);
   cta_sum_slots<36>(part_qz, b, e, red, Q);
-  cta_sum_slots<kNumRhs>(part_upd, b, e, red, rr);
+  cta_sum_slots<kNumRhs>(part_upd, sb[cell] * nsub, se[cell] * nsub, red, rr);
   if (threadIdx.x < 36) G[threadIdx.x] = B.g[threadIdx.x];
   __syncthreads();
   if (threadIdx.x != 0) return;
