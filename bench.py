@@ -473,6 +473,7 @@ def run_reference(args, world, rank):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded filtered-noise densities)",
         "impl": "reference", "config": workload_config(n, world),
         "precision": "FP64 throughout (CPU)",
+        "method": "the reference's: one multigrid PCG per load case (the GPU arm's V-cycle), no block CG",
         "timing": f"{len(secs)} full solve(s) timed (median), {warm} warm-up solve(s) of a 32^3 cell; "
                   f"requested --steps {args.steps} --warmup {args.warmup}",
         "cpu_baseline": {"value": 1.0 / sec, "unit": UNIT, "cores": cb["cores"], "kind": "port",
