@@ -12,7 +12,11 @@ without faulting the GPU (every error path ends in a status the host reads):
   handle in the same process solves correctly;
 * a device allocation that fails: FEMH_ARENA_LIMIT_BYTES caps a handle's
   set-up memory, the call reports FEMH_E_OOM, and a handle without the cap
-  solves correctly.
+  solves correctly;
+* a block PCG whose preconditioner is not positive definite (a damped-Jacobi
+  smoother with omega far above 2 / lambda_max): the block stops at its first
+  check and the cell is solved again one load case at a time, where the
+  one-case PCG falls back to Jacobi; the result is the one-case run's.
 The reference has no error reporting on this path beyond fem_error and printed
 PARDISO codes (femlib/include/femError.hpp:1-7, StepperCPU/src/pardiso_sym.cpp:60-68).
 """
@@ -106,3 +110,18 @@ def test_allocation_failure_reports_oom(femh, cell16, ref16, monkeypatch):
     f = femh.Engine()
     C, info = f.homogenize(cell16)
     assert info["status"] == 0 and _rel(C, ref16) < 1e-8
+
+
+def test_indefinite_block_falls_back_to_one_case_pcg(femh, cell16, ref16):
+    """omega = 1.9 without Chebyshev weights makes every sweep amplify the
+    high-frequency error, so the V-cycle is indefinite and z.r of the start is
+    not positive: the block reports CG_BLOCK_FAIL at once and the host solves
+    the cell one load case at a time (FP64: the very computation of block_cg=0,
+    the same iteration counts and the same C^H)."""
+    kw = dict(precision=femh.FP64, omega=1.9, cheb_ratio=0.0, pre_smooth=2, post_smooth=2, max_iter=5000)
+    Cb, ib = femh.Engine(block_cg=1, **kw).homogenize(cell16)
+    Cc, ic = femh.Engine(block_cg=0, **kw).homogenize(cell16)
+    assert ib["status"] == 0 and max(ib["rel_residual"]) < 1e-10
+    assert ib["iterations"] == ic["iterations"]
+    assert np.array_equal(Cb, Cc)
+    assert _rel(Cb, ref16) < 1e-8
