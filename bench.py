@@ -114,15 +114,24 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def engine_source_sha() -> str:
-    """Hash of the engine's device code (the kernel headers of fem_b200/csrc):
-    ties a DRAM-traffic capture to the kernels it measured."""
+# The headers a kernel family is compiled from: the stencil kernels include
+# only these two; every other kernel is hashed over all the headers.
+KERNEL_HEADERS = {"stencil_": ("femh_common.cuh", "stencil.cuh")}
+
+
+def engine_source_sha(kernel: str | None = None) -> str:
+    """Hash of the device code `kernel` is compiled from (the kernel headers of
+    fem_b200/csrc it includes; all of them when kernel is None): ties a
+    DRAM-traffic capture to the code it measured."""
     import hashlib
     h = hashlib.sha256()
     base = os.path.join(ROOT, "fem_b200", "csrc")
-    for f in sorted(os.listdir(base)):
-        if f.endswith(".cuh"):
-            h.update(open(os.path.join(base, f), "rb").read())
+    files = sorted(f for f in os.listdir(base) if f.endswith(".cuh"))
+    for prefix, hdrs in KERNEL_HEADERS.items():
+        if kernel is not None and kernel.startswith(prefix):
+            files = sorted(hdrs)
+    for f in files:
+        h.update(open(os.path.join(base, f), "rb").read())
     return h.hexdigest()[:16]
 
 
@@ -134,7 +143,7 @@ def kernel_traffic(kernel: str):
     if not os.path.exists(path):
         return None, "no ncu capture recorded"
     d = json.load(open(path))
-    if d.get("source_sha") != engine_source_sha():
+    if d.get("source_sha") != engine_source_sha(kernel):
         return None, "recorded ncu capture is of other engine sources"
     v = d.get("kernels", {}).get(kernel)
     return (v, d.get("how", "")) if v is not None else (None, f"no ncu capture of {kernel}")

@@ -622,7 +622,7 @@ __global__ void __launch_bounds__(256) k_bfin_beta(BlockCG* bst, CGState* stt, c
 // with ||r||^2 partials per load case ([sub-slot][6]) and, for the multigrid, the first
 // smoothing sweep z0 = omega D^-1 r and the residual copy rm of the V-cycle.
 // 256 threads; a node's new residuals wait in shared memory for the 3x3
-// node-block sweep (registers kept for three CTAs per SM).
+// node-block sweep (registers kept for three CTAs per SM: four measured slower).
 template <typename TV, typename TP, typename TQ, typename TZ>
 __global__ void __launch_bounds__(256, 3)
 k_bupdate(const CellDesc* cells, const NodeUnit* units, TV* __restrict__ x, TV* __restrict__ r,
@@ -692,7 +692,7 @@ k_bupdate(const CellDesc* cells, const NodeUnit* units, TV* __restrict__ x, TV* 
 
 // P = Z + P beta for the load cases of each live block (first: P = Z).
 template <typename TP, typename TZ>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)
 k_bdir(const CellDesc* cells, const NodeUnit* units, TP* __restrict__ p, const TZ* __restrict__ z,
        const BlockCG* bst, long long ntot, int first, int nsub) {
   const SubUnit su = sub_unit(units, nsub);
