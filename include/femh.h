@@ -80,7 +80,8 @@ typedef struct {
   int store_bf16;         /* mixed: bf16 storage of search directions and rho.  Converges on
                              small cells (<= 32^3 tested); on the 128^3 smooth and 256^3
                              binary benchmark cells CG then stalls near 1e-4 (the rounded
-                             search directions lose conjugacy): keep 0 there */
+                             search directions lose conjugacy): keep 0 there.  FEMH_MIXED_PC
+                             with block_cg keeps its search directions in FP64 regardless */
   int graph_chunk;        /* CG iterations per captured CUDA graph (0 = no graphs) */
   int coarse_avg;         /* coarse voxel modulus from its 8 children: 0 arithmetic mean
                              (rediscretisation of the mean), 1 geometric, 2 harmonic */
